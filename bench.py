@@ -1,0 +1,346 @@
+"""Benchmark of the fused LdG step (the QSR_cuda hot path) on B200.
+
+Default workload (one GPU): the anisotropic weak-anchoring relaxation -- 256^3 grid, droplet
+R = 120 cells, L1/L2/L3 = 6/3/1e-12 N, W = 1e-5 J/m^2, boundary_S = 0.6, T = 302 K, seeded random
+directors S0 = 0.5, explicit Euler at the reference's stable dt. A step is one explicit time
+step of the whole grid. ``value`` is box-cell-updates/s with the field resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs N independent replicas (one per GPU, no data-path collective; weak scaling).
+``--impl reference`` times the reference's own CPU step chain (QSR.cpp, built from the
+reference sources into oracle/_ref/) on the host cores, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LdG cell-updates/s"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL = 40  # FP32 SoA: 5 components read + 5 written per cell-update
+
+WORKLOADS = {
+    "anisotropic_weak_256": dict(
+        desc="256^3 droplet R=120 cells, L1/L2/L3=6/3/1e-12 N, W=1e-5 J/m^2 (boundary_S=0.6), T=302 K, "
+             "random directors S0=0.5 seed 42, explicit Euler at dt_max",
+        params=dict(Nx=256, Ny=256, Nz=256, dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6,
+                    T_star=307.0, bulk_modechoice=1, kappa=0.0, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5, gamma=0.1,
+                    droplet_radius_cells=120.0),
+        T=302.0, S_shell=0.6, S0=0.5, seed=42),
+    "plain_relaxation_64": dict(
+        desc="64^3 droplet R=28 cells, L1=6e-12 N, strong anchoring (equilibrium S_shell), T=300 K, "
+             "random directors S0=0.5 seed 42, explicit Euler at dt_max",
+        params=dict(Nx=64, Ny=64, Nz=64, dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6,
+                    T_star=307.0, bulk_modechoice=1, kappa=0.0, L1=6e-12, L2=0.0, L3=0.0, W=0.0, gamma=0.1,
+                    droplet_radius_cells=28.0),
+        T=300.0, S_shell=None, S0=0.5, seed=42),
+}
+DEFAULT_WORKLOAD = "anisotropic_weak_256"
+
+
+def dt_max(w):
+    from lcdrsimulator_b200.physics import DtRequest, estimate_stable_dt_window
+    p = w["params"]
+    r = DtRequest(dx=p["dx"], dy=p["dy"], dz=p["dz"], gamma=p["gamma"], a=p["a"], b=p["b"], c=p["c"],
+                  T_star=p["T_star"], modechoice=p["bulk_modechoice"], kappa=p["kappa"], L1=p["L1"], L2=p["L2"],
+                  L3=p["L3"], S0=w["S0"], T_a=w["T"], T_b=w["T"])
+    return estimate_stable_dt_window(r)["dt_max"]
+
+
+def shell_order(w):
+    from lcdrsimulator_b200.physics import equilibrium_shell_order
+    if w["S_shell"] is not None:
+        return w["S_shell"]
+    p = w["params"]
+    return equilibrium_shell_order(p["a"], p["b"], p["c"], w["T"], p["T_star"], p["bulk_modechoice"])
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_sample(w, target_s=12.0, grid=128, max_steps=400):
+    """The reference's own CPU step chain (QSR.cpp) on a bounded sample of the workload."""
+    from oracle.oracle import RefCPU, make_params
+    ref = RefCPU()
+    p = dict(w["params"])
+    p.update(Nx=grid, Ny=grid, Nz=grid, droplet_radius_cells=0.0)
+    op = make_params(**p)
+    rng = np.random.default_rng(w["seed"])
+    q = rng.normal(0.0, 0.2, grid ** 3 * 5)
+    dt = dt_max(w)
+    S_shell = shell_order(w)
+    t1 = ref.run_steps(op, q, w["T"], S_shell, dt, 1)  # warm-up and per-step estimate
+    n = int(max(2, min(max_steps, target_s / max(t1, 1e-6))))
+    t = ref.run_steps(op, q, w["T"], S_shell, dt, n)
+    cells = grid ** 3
+    return {"value": cells * n / t, "unit": UNIT, "cores": ref.max_threads(), "kind": "reference",
+            "sample": f"QSR.cpp step chain (computeLaplacian, computeChemicalPotential, applyWeakAnchoringPenalty, "
+                      f"updateQTensor, applyBoundaryConditions) on {grid}^3 with the workload's physics, "
+                      f"{n} steps, {t:.2f} s"}, t / n
+
+
+def run_reference_arm(args, w):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle.oracle import RefCPU
+    grid = args.ref_grid
+    cells = grid ** 3
+    from oracle.oracle import make_params
+    ref = RefCPU()
+    p = dict(w["params"])
+    p.update(Nx=grid, Ny=grid, Nz=grid, droplet_radius_cells=0.0)
+    op = make_params(**p)
+    q = np.random.default_rng(w["seed"]).normal(0.0, 0.2, cells * 5)
+    dt = dt_max(w)
+    S_shell = shell_order(w)
+    if args.warmup > 0:
+        ref.run_steps(op, q, w["T"], S_shell, dt, args.warmup)
+    t = ref.run_steps(op, q, w["T"], S_shell, dt, args.steps)
+    value = cells * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "desc": w["desc"], "sample_grid": [grid] * 3,
+                       "note": "the reference CPU path (QSR.cpp) on a bounded sample of the workload"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.max_threads(), "kind": "reference",
+                             "sample": f"{grid}^3 grid with the workload's physics, {args.steps} timed steps"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--ref-grid", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference_arm(args, w)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    import lcdrsimulator_b200 as L
+
+    solver = L.QSRSolver(**w["params"])
+    geo = solver.geometry()
+    q0 = solver.initial_field(0, w["seed"], w["S0"])
+    dt = dt_max(w)
+    S_shell = shell_order(w)
+    T = w["T"]
+    solver.upload(q0)
+    stream = torch.cuda.ExternalStream(solver.stream())
+
+    def barrier():
+        if pg is not None:
+            t = torch.ones(1, device="cuda")
+            pg.all_reduce(t)
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    args_step = solver.step_args(T, S_shell, dt)
+    for s in range(args.warmup):
+        args_step.step_index = s
+        solver.step_raw(1, args_step)
+    solver.sync()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    l0 = solver.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(args.steps):
+        args_step.step_index = args.warmup + s
+        solver.step_raw(1, args_step)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    barrier()
+    clocks = sampler.stop()
+    launches = solver.launch_count() - l0
+    ms = max_over_ranks(ms)
+    box = geo["box_cells"]
+    t_step = ms / 1e3 / args.steps
+    value = world * box * args.steps / (ms / 1e3)
+    touched = geo["active_cells"]
+    peak, peak_kind = load_peaks()
+    achieved = BYTES_PER_CELL * touched / t_step / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "qsr_step_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            tj = json.load(open(tfile))
+            traffic = tj.get("bytes_per_launch_full_size")
+        except Exception:
+            traffic = None
+
+    e2e = None
+    if not args.no_e2e:
+        # Drop-in run through the C ABI with host buffers: upload the field from pinned host
+        # memory, K steps with per-step host arguments, observables every 200 steps (the
+        # reference's print_freq default), download into pinned host memory.
+        q_in = torch.from_numpy(q0).pin_memory().numpy()
+        q_out = torch.empty(q0.size, dtype=torch.float64).pin_memory().numpy()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        solver.upload(q_in)
+        n_obs = 0
+        for s in range(args.steps):
+            args_step.step_index = s
+            solver.step_raw(1, args_step)
+            if s % 200 == 0:
+                solver.observe(T, S_shell)
+                n_obs += 1
+        solver.download(q_out)
+        e1.record(stream)
+        e1.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        barrier()
+        field_bytes = 5 * 8 * box
+        e2e = {"value": world * box * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": (field_bytes + args.steps * 72) / args.steps,
+               "d2h_bytes_per_step": (field_bytes + n_obs * 136) / args.steps,
+               "note": "qsr_upload (AoS FP64, pinned) + K x qsr_step + qsr_observe every 200 steps + qsr_download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_reference_sample(w)
+        except Exception as e:  # the reference build is test infrastructure; report its absence
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "grid": [w["params"]["Nx"], w["params"]["Ny"],
+                                                                            w["params"]["Nz"]],
+                       "box_cells": box, "active_cells": touched, "evolving_cells": geo["evolving_cells"],
+                       "active_cell_updates_per_s": world * touched * args.steps / (ms / 1e3),
+                       "dt_s": dt, "S_shell": S_shell, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (two 5-component FP32 fields of 335 MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "bytes_per_cell_update": BYTES_PER_CELL, "kernel_ms": t_step * 1e3},
+            "clocks": clocks,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

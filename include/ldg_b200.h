@@ -1,0 +1,176 @@
+/*
+ * ldg_b200.h -- C ABI of the B200 Landau-de Gennes Q-tensor solver library (libldg_b200.so).
+ *
+ * The reference (Spectre71/LCDrSimulator) has no library API: its programs QSR_cuda and
+ * KZM_bulk_ldg_cuda launch their kernels directly from main(). Each entry point below
+ * replaces one block of that main() and cites it. All entry points:
+ *   - take plain pointers and sizes (no C++ or torch types);
+ *   - return int status (LDG_OK = 0, LDG_ERR_* otherwise) and never exit or prompt;
+ *   - record a message for ldg_last_error() (thread-local) on failure;
+ *   - enqueue work on one CUDA stream owned by the handle. qsr_step/kzm_step return after
+ *     enqueueing; observe/download/nematic synchronise the stream before returning.
+ * A handle must be used from one host thread at a time.
+ *
+ * Host field layout at the boundary is the reference's: AoS FP64, 5 doubles per cell
+ * (Qxx, Qxy, Qxz, Qyy, Qyz), QSR.cuh:22 / KZM_bulk_ldg.cuh:9. Cell order is
+ * k + Nz*(j + Ny*i) for the confined solver (QSR.cu:286) and x + Nx*(y + Ny*z) for the
+ * periodic bulk solver (KZM_bulk_ldg.cu:161-169). On the device the field is FP32 SoA.
+ */
+#ifndef LDG_B200_H
+#define LDG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDG_OK 0
+#define LDG_ERR_ARG 1        /* invalid argument or size                        */
+#define LDG_ERR_CUDA 2       /* CUDA runtime error (message has the CUDA string) */
+#define LDG_ERR_NONFINITE 3  /* a reduction saw a non-finite field value        */
+#define LDG_ERR_TIMEOUT 4    /* a bounded device wait gave up                    */
+#define LDG_ERR_STATE 5      /* call out of order (e.g. step before upload)      */
+#define LDG_ERR_NOMEM 6      /* device allocation failed                         */
+
+/* ------------------------------------------------------------------------------------
+ * Confined droplet solver (QSR_cuda)
+ * ------------------------------------------------------------------------------------ */
+typedef struct qsr_params {
+    int Nx, Ny, Nz;                 /* grid, each >= 3 (QSR.cu:1966-1968)                     */
+    double dx, dy, dz;              /* spacing in m (QSR.cu:1969-1971)                        */
+    double a, b, c, T_star;         /* LdG constants (QSR.cu:1974-1978)                       */
+    int bulk_modechoice;            /* 1 = std, 2 = ravnik (QSR.cu:1979, 385-397)             */
+    double kappa;                   /* one-constant elastic, used when L1 = L2 = L3 = 0       */
+    double L1, L2, L3;              /* anisotropic elastic constants (QSR.cu:2057-2060)       */
+    double W;                       /* anchoring: 0 strong, > 0 Rapini-Papoular (QSR.cu:2113) */
+    double gamma;                   /* rotational viscosity (QSR.cu:2114)                     */
+    double droplet_radius_cells;    /* <= 0: reference radius 0.5*(min(N)-1) (QSR.cu:151)     */
+} qsr_params;
+
+typedef struct qsr_geometry_info {
+    double center_x, center_y, center_z;
+    double radius_x, radius_y, radius_z;
+    double min_spacing, shell_half_thickness;
+    double delta_eff;               /* shell volume / ellipsoid area (QSR.cu:174-185)         */
+    long long shell_cells;          /* cells with |sd| <= shell_half_thickness                */
+    long long evolving_cells;       /* cells the update touches                               */
+    long long active_cells;         /* cells in tiles the step kernel visits                  */
+    long long box_cells;            /* Nx*Ny*Nz                                               */
+} qsr_geometry_info;
+
+typedef struct qsr_step_args {
+    double T;                       /* temperature of this step (QSR.cu:2709)                 */
+    double S_shell;                 /* shell order of this step (QSR.cu:2711, 1475-1487)      */
+    double dt;                      /* time step (QSR.cu:2575-2576)                           */
+    double q_norm_cap;              /* 0: off; Frobenius cap of the explicit update (2608)    */
+    double noise_sigma;             /* 0: off; Langevin amplitude per component per step      */
+    unsigned long long seed;        /* Philox key for the noise                               */
+    long long step_index;           /* global index of the first step (noise counter)         */
+    int semi_implicit;              /* 1: IMEX Helmholtz-Jacobi update (QSR.cu:2721-2749)     */
+    double L_stab;                  /* IMEX stabiliser coefficient                            */
+    int jacobi_iters;               /* IMEX Jacobi sweeps per step                            */
+} qsr_step_args;
+
+typedef struct qsr_observe_args {
+    double T, S_shell;              /* state the energy is evaluated at                       */
+    int defects_z_slice;            /* slice of the 2-D defect proxy and checker metric       */
+    double defects_S_threshold;     /* default 0.1  (QSR.cu:2634-2644)                        */
+    double defects_charge_cutoff;   /* default 0.25                                           */
+    int xi_z_slice;                 /* slice of the xi-gradient proxy                         */
+    double xi_S_threshold;
+    int want_defects;               /* 0 skips the 2-D defect proxy                           */
+    int want_xi;                    /* 0 skips the xi proxy                                   */
+} qsr_observe_args;
+
+typedef struct qsr_observables {
+    double bulk, elastic, anchoring, total;          /* J (QSR.cu:869-992, 654-695)           */
+    double radiality; long long radiality_count;     /* QSR.cu:994-1015                       */
+    double avg_S, max_S; long long core_count;       /* QSR.cu:2285-2321                      */
+    double checker_rel;                              /* NaN unless max_S >= 0.5 (2839-2873)   */
+    double defect_density;                           /* NaN when no plaquette (2343-2364)     */
+    long long defect_count, defect_plaquettes;
+    double xi_grad_proxy; long long xi_edges;        /* QSR.cu:2372-2410                      */
+    double max_q_norm;                               /* max Frobenius norm |Q| (debug_dynamics) */
+    long long nonfinite_cells;                       /* cells with a non-finite component     */
+} qsr_observables;
+
+typedef struct qsr_handle qsr_handle;
+
+/* Replaces the setup block QSR.cu:2141-2226: geometry in FP64, shell mask, delta_eff,
+ * device allocations. */
+int qsr_create(const qsr_params* params, qsr_handle** out);
+int qsr_geometry(const qsr_handle* h, qsr_geometry_info* out);
+/* Replaces initializeQTensor / initializeIsotropicWithNoise (QSR.cu:1834-1904): writes the
+ * reference's seeded initial field into q_aos5 (host). init_mode 0 random directors, 1 radial,
+ * 2 isotropic + N(0, noise_amplitude); std::mt19937(random_seed), random_device if seed < 0. */
+int qsr_initial_field(const qsr_handle* h, int init_mode, long long random_seed, double S0,
+                      double noise_amplitude, double* q_aos5);
+/* Replaces cudaMemcpy H2D of the initial field (QSR.cu:2515, 3078, 3185). */
+int qsr_upload(qsr_handle* h, const double* q_aos5);
+/* Replaces the D2H of the final / snapshot field (QSR.cu:2930, 2974, 3469). */
+int qsr_download(qsr_handle* h, double* q_aos5);
+/* Replaces n_steps iterations of the per-step kernel chain: Laplacian, divergence,
+ * chemical potential, L3, weak anchoring, update or IMEX, boundary conditions
+ * (QSR.cu:2713-2753, 3079-3088, 3234-3249). */
+int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* args);
+/* Replaces the log-point observables: reduce_energy (QSR.cu:2323-2341), radiality
+ * (2788-2802), nematic avg/max S and checker (2285-2321, 2827-2874), defect proxy
+ * (2343-2364) and xi proxy (2372-2410). FP64 reductions, deterministic. */
+int qsr_observe(qsr_handle* h, const qsr_observe_args* args, qsr_observables* out);
+/* Replaces computeNematicFieldKernel + D2H (QSR.cu:1017-1025, 2816-2821): 4 doubles per
+ * cell (S, nx, ny, nz) in the host cell order. */
+int qsr_nematic(qsr_handle* h, double* s_n4);
+int qsr_sync(qsr_handle* h);
+/* The handle's CUDA stream (a cudaStream_t), for timing with events. */
+void* qsr_stream(qsr_handle* h);
+/* Kernels launched by this handle since creation (launch counter). */
+long long qsr_launch_count(const qsr_handle* h);
+int qsr_destroy(qsr_handle* h);
+
+/* ------------------------------------------------------------------------------------
+ * Periodic bulk solver (KZM_bulk_ldg_cuda)
+ * ------------------------------------------------------------------------------------ */
+typedef struct kzm_params {
+    int Nx, Ny, Nz;                 /* each > 1 (KZM_bulk_ldg.cu:824-826)                     */
+    double dx, dy, dz;
+    double kappa, gamma;            /* one-constant elastic and viscosity                     */
+    double q_norm_cap;              /* 0: off (KZM_bulk_ldg.cu:456-467)                       */
+    double defects_S_threshold, defects_charge_cutoff;
+} kzm_params;
+
+typedef struct kzm_step_args {
+    double A, B, C;                 /* bulk coefficients at this step (KZM_bulk_ldg.cu:919-921) */
+    double dt;
+    double noise_sigma;             /* sqrt(2/gamma*noise_strength*dt) (KZM_bulk_ldg.cu:955)  */
+    unsigned long long seed;
+    long long step_index;           /* iteration of the first step (noise counter)           */
+} kzm_step_args;
+
+typedef struct kzm_observables {
+    double bulk, elastic, total;                     /* per volume (KZM_bulk_ldg.cu:694-696)  */
+    double avg_S, max_S;
+    double defect_density_per_plaquette, defect_line_density, xi_grad_proxy;
+    long long defect_plaquettes_used, nonzero_defect_plaquettes;
+} kzm_observables;
+
+typedef struct kzm_handle kzm_handle;
+
+/* Replaces KZM_bulk_ldg.cu:895-899 (allocation and upload of the field). */
+int kzm_create(const kzm_params* params, kzm_handle** out);
+int kzm_upload(kzm_handle* h, const double* q_aos5);
+int kzm_download(kzm_handle* h, double* q_aos5);
+/* Replaces n_steps iterations of updateBulkLdgKernel + swap (KZM_bulk_ldg.cu:951-970). */
+int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* args);
+/* Replaces the full D2H + host compute_observables (KZM_bulk_ldg.cu:923-925, 543-713). */
+int kzm_observe(kzm_handle* h, double A, double B, double C, kzm_observables* out);
+void* kzm_stream(kzm_handle* h);
+long long kzm_launch_count(const kzm_handle* h);
+int kzm_destroy(kzm_handle* h);
+
+/* ------------------------------------------------------------------------------------ */
+const char* ldg_last_error(void);
+const char* ldg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

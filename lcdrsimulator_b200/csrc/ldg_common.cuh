@@ -1,0 +1,356 @@
+// Shared device code of the B200 LdG solver: field layout, per-cell physics written
+// against a neighbour accessor, the counter-based noise generator and the FP64 nematic
+// eigen-solver used by the reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ldg {
+
+// Per-cell classification bits, computed once on the host in FP64 (qsr.cu) from the
+// reference predicates (QSR.cu:100-111, 697-709, 851-867, 994-1002, 2288-2300).
+enum : uint8_t {
+    kMove = 1,     // the update touches the cell: !(W == 0 && shell) && sd <= band
+    kFixed = 2,    // strong anchoring: W <= 0 && shell, rewritten to Q0 after the update
+    kAnchor = 4,   // weak anchoring penalty: shell && W != 0 && delta_eff > 0
+    kShell = 8,    // |sd| <= shell half thickness
+    kInside = 16,  // sd <= 0
+    kCore = 32,    // sd < -2 min_spacing (avg_S, max_S, checker)
+    kRadial = 64,  // inside && |r| > 2 min_spacing (radiality)
+};
+
+// Constants of one confined-solver step, passed by value to the kernels. The field is
+// FP32 SoA: component c of cell (i, j, k) lives at q[c*sc + i*si + j*sj + k].
+struct QsrConst {
+    int Nx, Ny, Nz;
+    int sj;          // row pitch (>= Nz, multiple of 4)
+    long long si;    // plane pitch = Ny*sj
+    long long sc;    // component pitch = Nx*si
+    float ix2, iy2, iz2;        // 1/d^2
+    float i2x, i2y, i2z;        // 1/(2d)
+    float ix, iy, iz;           // 1/d
+    float i4xy, i4xz, i4yz;     // 1/(4 da db)
+    float cQ, cQ2, cQ3;         // bulk force coefficients (QSR.cu:385-397)
+    float Liso;                 // kappa if L1 = L2 = L3 = 0, else L1 (QSR.cu:420-438)
+    float L2, L3;
+    float Weff, S_shell;        // W/delta_eff and the shell order
+    float mob_dt;               // dt/gamma
+    float qcap;                 // Frobenius cap (0 = off)
+    float ci, cj, ck;           // droplet centre in cell units, (N-1)/2
+    float gnx, gny, gnz;        // d/r^2 per axis: surface normal ~ (X gnx, Y gny, Z gnz)
+    float sigma;                // Langevin amplitude per component (0 = off)
+    uint32_t key0, key1;        // Philox key (seed)
+    uint32_t instance;          // ensemble instance id (noise counter word)
+    long long step;             // global step index (noise counter words)
+    // semi-implicit (IMEX) Helmholtz-Jacobi
+    float alpha;                // (dt/gamma) L_stab
+    float jdenom_inv;           // 1/(1 + 2 alpha sum 1/d^2)
+};
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) and Box-Muller normals.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]);
+        const uint32_t lo0 = 0xD2511F53u * c[0];
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const uint32_t lo1 = 0xCD9E8D57u * c[2];
+        const uint32_t n0 = hi1 ^ c[1] ^ k0;
+        const uint32_t n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+// Uniform in (0, 1] from the top 24 bits.
+__device__ __forceinline__ float u01(uint32_t x) { return ((float)(x >> 8) + 1.0f) * (1.0f / 16777216.0f); }
+
+// Five standard normals for (cell, instance, step): two Philox blocks, Box-Muller pairs.
+__device__ __forceinline__ void normals5(uint32_t cell, uint32_t instance, long long step, uint32_t k0, uint32_t k1,
+                                         float g[5]) {
+    float z[8];
+#pragma unroll
+    for (int blk = 0; blk < 2; ++blk) {
+        uint32_t c[4] = {cell, instance, (uint32_t)step, ((uint32_t)((unsigned long long)step >> 32) << 1) | (uint32_t)blk};
+        philox4x32_10(c, k0, k1);
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const float r = sqrtf(-2.0f * logf(u01(c[2 * p])));
+            float s, co;
+            sincospif(2.0f * u01(c[2 * p + 1]), &s, &co);
+            z[4 * blk + 2 * p] = r * co;
+            z[4 * blk + 2 * p + 1] = r * s;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) g[m] = z[m];
+}
+
+// ---------------------------------------------------------------------------------------
+// Stencil physics. `A(c, di, dj, dk)` returns component c (0..4, 5 = Qzz) of the cell at
+// offset (di, dj, dk); the face logic below never asks for a cell outside the grid.
+// ---------------------------------------------------------------------------------------
+
+// Second derivative along one axis with the reference's shifted stencil at the faces
+// (QSR.cu:296-320).
+template <int AX, class Acc>
+__device__ __forceinline__ float d2_face(const Acc& A, int c, float cv, int pos, int n, float inv) {
+    auto at = [&](int s) { return AX == 0 ? A(c, s, 0, 0) : (AX == 1 ? A(c, 0, s, 0) : A(c, 0, 0, s)); };
+    if (pos > 0 && pos < n - 1) return (at(1) - cv * 2.0f + at(-1)) * inv;
+    if (pos == 0) return (at(2) - at(1) * 2.0f + cv) * inv;
+    return (cv - at(-1) * 2.0f + at(-2)) * inv;
+}
+
+// First derivative along one axis at offset (oi, oj, ok), one-sided first order at the faces
+// (QSR.cu:245-273). `pos` is the absolute coordinate of the offset cell along AX.
+template <int AX, class Acc>
+__device__ __forceinline__ float d1_face(const Acc& A, int c, int oi, int oj, int ok, int pos, int n, float i2, float i1) {
+    auto at = [&](int s) {
+        return AX == 0 ? A(c, oi + s, oj, ok) : (AX == 1 ? A(c, oi, oj + s, ok) : A(c, oi, oj, ok + s));
+    };
+    if (pos > 0 && pos < n - 1) return (at(1) - at(-1)) * i2;
+    if (pos == 0) return (at(1) - at(0)) * i1;
+    return (at(0) - at(-1)) * i1;
+}
+
+// Column divergence D_j = d_k Q_kj at offset (oi, oj, ok) of cell (i, j, k) (QSR.cu:325-371).
+template <class Acc>
+__device__ __forceinline__ void dcol_at(const Acc& A, const QsrConst& P, int i, int j, int k, int oi, int oj, int ok,
+                                        float D[3]) {
+    const int pi = i + oi, pj = j + oj, pk = k + ok;
+    D[0] = d1_face<0>(A, 0, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 1, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2>(A, 2, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+    D[1] = d1_face<0>(A, 1, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 3, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2>(A, 4, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+    D[2] = d1_face<0>(A, 2, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 4, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2>(A, 5, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+}
+
+// Bulk molecular field entries xx yy zz xy xz yz (QSR.cu:399-417).
+__device__ __forceinline__ void bulk_field(const float q[5], float cQ, float cQ2, float cQ3, float h[6]) {
+    const float Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4];
+    const float Qzz = -Qxx - Qyy;
+    const float trQ2 = Qxx * Qxx + Qyy * Qyy + Qzz * Qzz + 2.0f * (Qxy * Qxy + Qxz * Qxz + Qyz * Qyz);
+    const float q2xx = Qxx * Qxx + Qxy * Qxy + Qxz * Qxz;
+    const float q2xy = Qxx * Qxy + Qxy * Qyy + Qxz * Qyz;
+    const float q2xz = Qxx * Qxz + Qxy * Qyz + Qxz * Qzz;
+    const float q2yy = Qxy * Qxy + Qyy * Qyy + Qyz * Qyz;
+    const float q2yz = Qxy * Qxz + Qyy * Qyz + Qyz * Qzz;
+    const float q2zz = Qxz * Qxz + Qyz * Qyz + Qzz * Qzz;
+    const float t3 = trQ2 / 3.0f;
+    const float g = cQ3 * trQ2;
+    h[0] = cQ * Qxx - cQ2 * (q2xx - t3) + g * Qxx;
+    h[1] = cQ * Qyy - cQ2 * (q2yy - t3) + g * Qyy;
+    h[2] = cQ * Qzz - cQ2 * (q2zz - t3) + g * Qzz;
+    h[3] = cQ * Qxy - cQ2 * q2xy + g * Qxy;
+    h[4] = cQ * Qxz - cQ2 * q2xz + g * Qxz;
+    h[5] = cQ * Qyz - cQ2 * q2yz + g * Qyz;
+}
+
+// Droplet surface normal at cell (i, j, k) (QSR.cu:130-142), in FP32 from cell units.
+__device__ __forceinline__ void surface_q0(const QsrConst& P, int i, int j, int k, float Q0[5]) {
+    const float gx = ((float)i - P.ci) * P.gnx, gy = ((float)j - P.cj) * P.gny, gz = ((float)k - P.ck) * P.gnz;
+    const float gn = sqrtf(gx * gx + gy * gy + gz * gz);
+    float nx = 1.0f, ny = 0.0f, nz = 0.0f;
+    if (gn > 0.0f) { nx = gx / gn; ny = gy / gn; nz = gz / gn; }
+    const float S = P.S_shell;
+    Q0[0] = S * (nx * nx - 1.0f / 3.0f);
+    Q0[1] = S * (nx * ny);
+    Q0[2] = S * (nx * nz);
+    Q0[3] = S * (ny * ny - 1.0f / 3.0f);
+    Q0[4] = S * (ny * nz);
+}
+
+// Chemical potential of cell (i, j, k): bulk + elastic (iso | L1, L2) projected traceless,
+// then L3 on interior cells re-projected, then the weak-anchoring penalty
+// (QSR.cu:373-472, 474-621, 623-652). `lap` returns the Laplacian (IMEX uses it).
+// DAcc(c, di, dj, dk) returns the column divergence D_c at a face-neighbour offset.
+template <bool kL2, bool kL3, class Acc, class DAcc>
+__device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, const QsrConst& P, int i, int j, int k,
+                                               const float q[5], bool anchor, float mu[5], float lap[5]) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const float d2x = d2_face<0>(A, c, q[c], i, P.Nx, P.ix2);
+        const float d2y = d2_face<1>(A, c, q[c], j, P.Ny, P.iy2);
+        const float d2z = d2_face<2>(A, c, q[c], k, P.Nz, P.iz2);
+        lap[c] = d2x + d2y + d2z;
+    }
+    float h[6];
+    bulk_field(q, P.cQ, P.cQ2, P.cQ3, h);
+    const float lzz = -lap[0] - lap[3];
+    h[0] -= P.Liso * lap[0];
+    h[1] -= P.Liso * lap[3];
+    h[2] -= P.Liso * lzz;
+    h[3] -= P.Liso * lap[1];
+    h[4] -= P.Liso * lap[2];
+    h[5] -= P.Liso * lap[4];
+    if (kL2) {
+        // d_a D_b with one-sided faces (QSR.cu:436-460).
+        auto dD = [&](int comp, int ax) {
+            const int pos = ax == 0 ? i : (ax == 1 ? j : k);
+            const int n = ax == 0 ? P.Nx : (ax == 1 ? P.Ny : P.Nz);
+            const float i2 = ax == 0 ? P.i2x : (ax == 1 ? P.i2y : P.i2z);
+            const float i1 = ax == 0 ? P.ix : (ax == 1 ? P.iy : P.iz);
+            auto at = [&](int s) {
+                return ax == 0 ? DA(comp, s, 0, 0) : (ax == 1 ? DA(comp, 0, s, 0) : DA(comp, 0, 0, s));
+            };
+            if (pos > 0 && pos < n - 1) return (at(1) - at(-1)) * i2;
+            if (pos == 0) return (at(1) - at(0)) * i1;
+            return (at(0) - at(-1)) * i1;
+        };
+        const float L2 = P.L2;
+        h[0] -= L2 * dD(0, 0);
+        h[1] -= L2 * dD(1, 1);
+        h[2] -= L2 * dD(2, 2);
+        h[3] -= L2 * (dD(1, 0) + dD(0, 1));
+        h[4] -= L2 * (dD(2, 0) + dD(0, 2));
+        h[5] -= L2 * (dD(2, 1) + dD(1, 2));
+    }
+    float corr = (h[0] + h[1] + h[2]) / 3.0f;
+    mu[0] = h[0] - corr;
+    mu[1] = h[3];
+    mu[2] = h[4];
+    mu[3] = h[1] - corr;
+    mu[4] = h[5];
+    if (kL3) {
+        const bool interior = (i > 0 && i < P.Nx - 1 && j > 0 && j < P.Ny - 1 && k > 0 && k < P.Nz - 1);
+        if (interior) {
+            float hx[6] = {mu[0], mu[3], -(mu[0] + mu[3]), mu[1], mu[2], mu[4]};
+            float d[6][3];
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                d[c][0] = (A(c, 1, 0, 0) - A(c, -1, 0, 0)) * P.i2x;
+                d[c][1] = (A(c, 0, 1, 0) - A(c, 0, -1, 0)) * P.i2y;
+                d[c][2] = (A(c, 0, 0, 1) - A(c, 0, 0, -1)) * P.i2z;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) d[5][a] = -(d[0][a] + d[3][a]);
+            auto M = [&](int a, int b) {
+                return d[0][a] * d[0][b] + d[3][a] * d[3][b] + d[5][a] * d[5][b] +
+                       2.0f * (d[1][a] * d[1][b] + d[2][a] * d[2][b] + d[4][a] * d[4][b]);
+            };
+            const float hl3 = 0.5f * P.L3;
+            hx[0] += hl3 * M(0, 0);
+            hx[1] += hl3 * M(1, 1);
+            hx[2] += hl3 * M(2, 2);
+            hx[3] += hl3 * M(0, 1);
+            hx[4] += hl3 * M(0, 2);
+            hx[5] += hl3 * M(1, 2);
+            const float Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4], Qzz = -q[0] - q[3];
+            const float Dc0 = DA(0, 0, 0, 0), Dc1 = DA(1, 0, 0, 0), Dc2 = DA(2, 0, 0, 0);
+            // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603).
+            auto Bc = [&](int c) {
+                const float Qc = c == 5 ? Qzz : q[c];
+                const float d2xx = (A(c, 1, 0, 0) - 2.0f * Qc + A(c, -1, 0, 0)) * P.ix2;
+                const float d2yy = (A(c, 0, 1, 0) - 2.0f * Qc + A(c, 0, -1, 0)) * P.iy2;
+                const float d2zz = (A(c, 0, 0, 1) - 2.0f * Qc + A(c, 0, 0, -1)) * P.iz2;
+                const float d2xy = (A(c, 1, 1, 0) - A(c, 1, -1, 0) - A(c, -1, 1, 0) + A(c, -1, -1, 0)) * P.i4xy;
+                const float d2xz = (A(c, 1, 0, 1) - A(c, 1, 0, -1) - A(c, -1, 0, 1) + A(c, -1, 0, -1)) * P.i4xz;
+                const float d2yz = (A(c, 0, 1, 1) - A(c, 0, 1, -1) - A(c, 0, -1, 1) + A(c, 0, -1, -1)) * P.i4yz;
+                const float contract = Qxx * d2xx + Qyy * d2yy + Qzz * d2zz + 2.0f * (Qxy * d2xy + Qxz * d2xz + Qyz * d2yz);
+                return Dc0 * d[c][0] + Dc1 * d[c][1] + Dc2 * d[c][2] + contract;
+            };
+            const float Bxx = Bc(0), Byy = Bc(3), Bzz = -(Bxx + Byy);
+            const float Bxy = Bc(1), Bxz = Bc(2), Byz = Bc(4);
+            hx[0] -= P.L3 * Bxx;
+            hx[1] -= P.L3 * Byy;
+            hx[2] -= P.L3 * Bzz;
+            hx[3] -= P.L3 * Bxy;
+            hx[4] -= P.L3 * Bxz;
+            hx[5] -= P.L3 * Byz;
+            corr = (hx[0] + hx[1] + hx[2]) / 3.0f;
+            mu[0] = hx[0] - corr;
+            mu[3] = hx[1] - corr;
+            mu[1] = hx[3];
+            mu[2] = hx[4];
+            mu[4] = hx[5];
+        }
+    }
+    if (anchor) {
+        float Q0[5];
+        surface_q0(P, i, j, k, Q0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) mu[c] += P.Weff * (q[c] - Q0[c]);
+    }
+}
+
+// Explicit Euler update with optional Langevin noise and Frobenius cap (QSR.cu:711-731).
+__device__ __forceinline__ void euler_update(const QsrConst& P, const float q[5], const float mu[5], uint32_t cell,
+                                             bool noise, float out[5]) {
+#pragma unroll
+    for (int c = 0; c < 5; ++c) out[c] = q[c] - mu[c] * P.mob_dt;
+    if (noise) {
+        float g[5];
+        normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) out[c] += P.sigma * g[c];
+    }
+    if (P.qcap > 0.0f) {
+        const float zz = -out[0] - out[3];
+        const float tr = out[0] * out[0] + out[3] * out[3] + zz * zz +
+                         2.0f * (out[1] * out[1] + out[2] * out[2] + out[4] * out[4]);
+        const float qn = sqrtf(tr > 0.0f ? tr : 0.0f);
+        if (qn > P.qcap && qn > 0.0f) {
+            const float s = P.qcap / qn;
+#pragma unroll
+            for (int c = 0; c < 5; ++c) out[c] *= s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// FP64 nematic eigen-solver (QSR.cu:191-243): shifted power iteration for the largest
+// eigenvalue, S = 1.5 lambda, director gauge nz >= 0.
+// ---------------------------------------------------------------------------------------
+struct Nematic { double S, nx, ny, nz; };
+
+__device__ __forceinline__ Nematic nematic64(const double q[5], double iso_cut, Nematic iso) {
+    const double Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4];
+    const double Qzz = -Qxx - Qyy;
+    if (fabs(Qxx) < iso_cut && fabs(Qxy) < iso_cut && fabs(Qxz) < iso_cut && fabs(Qyy) < iso_cut &&
+        fabs(Qyz) < iso_cut)
+        return iso;
+    double nx = Qxx + Qxy + Qxz, ny = Qxy + Qyy + Qyz, nz = Qxz + Qyz - Qxx - Qyy;
+    const double n0 = sqrt(nx * nx + ny * ny + nz * nz);
+    if (n0 > 1e-12) { nx /= n0; ny /= n0; nz /= n0; }
+    else { nx = 0.0; ny = 0.0; nz = 1.0; }
+    const double r1 = fabs(Qxx) + fabs(Qxy) + fabs(Qxz);
+    const double r2 = fabs(Qxy) + fabs(Qyy) + fabs(Qyz);
+    const double r3 = fabs(Qxz) + fabs(Qyz) + fabs(Qzz);
+    const double alpha = fmax(r1, fmax(r2, r3)) + 1e-12;
+    for (int it = 0; it < 15; ++it) {
+        const double ax = Qxx * nx + Qxy * ny + Qxz * nz + alpha * nx;
+        const double ay = Qxy * nx + Qyy * ny + Qyz * nz + alpha * ny;
+        const double az = Qxz * nx + Qyz * ny + Qzz * nz + alpha * nz;
+        const double nn = sqrt(ax * ax + ay * ay + az * az);
+        if (nn < 1e-13) break;
+        nx = ax / nn; ny = ay / nn; nz = az / nn;
+    }
+    const double lam = nx * (Qxx * nx + Qxy * ny + Qxz * nz) + ny * (Qxy * nx + Qyy * ny + Qyz * nz) +
+                       nz * (Qxz * nx + Qyz * ny + Qzz * nz);
+    Nematic r{1.5 * lam, nx, ny, nz};
+    if (nz < -1e-10) { r.nx = -nx; r.ny = -ny; r.nz = -nz; }
+    return r;
+}
+
+// Warp and block reductions (fixed order: deterministic for a fixed launch shape).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+}  // namespace ldg

@@ -1,0 +1,169 @@
+"""GPU parity of the confined-droplet CUDA path against the FP64 oracle, through the C ABI.
+
+Tolerances (FP32 device fields vs FP64 oracle, relative to max |Q|):
+  * a few explicit steps from an identical FP32-representable field: <= 2e-6
+  * 2000 explicit steps (32^3, L1, strong anchoring): field <= 1e-5, free energy <= 1e-6
+  * FP64 reductions on an identical FP32-representable field: energies <= 1e-10 relative,
+    integer counts exact.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from gpu_helpers import make_pair, fp32, rel_err, rms_rel
+from lcdrsimulator_b200.physics import bulk_ABC, S_eq, estimate_stable_dt_window, DtRequest
+
+pytestmark = pytest.mark.gpu
+
+STEP_CASES = {
+    "L1_strong": dict(Nx=32, Ny=32, Nz=32, L1=6e-12),
+    "kappa_strong": dict(Nx=24, Ny=24, Nz=24, L1=0.0, kappa=6.5e-12),
+    "L1L2L3_weak": dict(Nx=24, Ny=20, Nz=28, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5),
+    "ravnik_L3_weak": dict(Nx=20, Ny=20, Nz=20, bulk_modechoice=2, L1=6e-12, L3=2e-12, W=1e-5),
+    "aniso_spacing_L2": dict(Nx=20, Ny=24, Nz=18, dy=1.2e-8, dz=0.9e-8, L1=6e-12, L2=2e-12, W=2e-5),
+    "odd_grid_all_terms": dict(Nx=13, Ny=11, Nz=9, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5),
+    "radius_override_weak": dict(Nx=32, Ny=32, Nz=32, droplet_radius_cells=10.0, L1=6e-12, W=1e-5),
+    "minimum_grid_3": dict(Nx=3, Ny=3, Nz=3, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5),
+    "negative_W": dict(Nx=16, Ny=16, Nz=16, L1=6e-12, W=-1e-6),
+}
+
+
+def _dt(d, T):
+    r = DtRequest(dx=d["dx"], dy=d["dy"], dz=d["dz"], gamma=d["gamma"], a=d["a"], b=d["b"], c=d["c"],
+                  T_star=d["T_star"], modechoice=d["bulk_modechoice"], kappa=d["kappa"], L1=d["L1"], L2=d["L2"],
+                  L3=d["L3"], S0=0.5, T_a=T, T_b=T)
+    return estimate_stable_dt_window(r)["dt_max"]
+
+
+@pytest.mark.parametrize("name", list(STEP_CASES))
+def test_explicit_steps_match_oracle(oracle, name):
+    op, solver, d = make_pair(**STEP_CASES[name])
+    g, fl = oracle.geometry(op)
+    geo = solver.geometry()
+    assert geo["shell_cells"] == g.shell_count
+    assert geo["delta_eff"] == pytest.approx(g.delta_eff, rel=1e-14)
+    T, S_shell = 302.0, 0.6
+    q0 = fp32(oracle.init(op, g, 0, 42, 0.5))
+    dt = _dt(d, T)
+    solver.upload(q0)
+    solver.step(5, T, S_shell, dt)
+    got = solver.download()
+    want = oracle.step_explicit(op, g, fl, q0, T, S_shell, dt, n=5)
+    assert rel_err(got, want) <= 2e-6, (name, rel_err(got, want))
+    solver.close()
+
+
+def test_q_norm_cap_matches_oracle(oracle):
+    op, solver, d = make_pair(Nx=16, Ny=16, Nz=16, L1=6e-12)
+    g, fl = oracle.geometry(op)
+    q0 = fp32(oracle.init(op, g, 0, 5, 1.1))
+    cap = 1.0 * math.sqrt(2.0 / 3.0)
+    dt = _dt(d, 300.0)
+    solver.upload(q0)
+    solver.step(3, 300.0, 0.9, dt, q_norm_cap=cap)
+    want = oracle.step_explicit(op, g, fl, q0, 300.0, 0.9, dt, q_norm_cap=cap, n=3)
+    assert rel_err(solver.download(), want) <= 2e-6
+
+
+@pytest.mark.parametrize("name", ["L1_strong", "L1L2L3_weak", "odd_grid_all_terms"])
+def test_imex_steps_match_oracle(oracle, name):
+    op, solver, d = make_pair(**STEP_CASES[name])
+    g, fl = oracle.geometry(op)
+    q0 = fp32(oracle.init(op, g, 0, 7, 0.5))
+    T, S_shell, L_stab, iters = 301.0, 0.6, d["L1"], 25
+    dt = 4 * _dt(d, T)
+    solver.upload(q0)
+    solver.step(3, T, S_shell, dt, semi_implicit=True, L_stab=L_stab, jacobi_iters=iters)
+    want = oracle.step_imex(op, g, fl, q0, T, S_shell, dt, L_stab, iters, n=3)
+    assert rel_err(solver.download(), want) <= 2e-6
+
+
+@pytest.mark.parametrize("name", ["L1_strong", "L1L2L3_weak", "radius_override_weak", "odd_grid_all_terms"])
+def test_observables_match_oracle_on_identical_field(oracle, name):
+    op, solver, d = make_pair(**STEP_CASES[name])
+    g, fl = oracle.geometry(op)
+    q = oracle.init(op, g, 0, 9, 0.6)
+    q = fp32(oracle.step_explicit(op, g, fl, q, 300.0, 0.6, _dt(d, 300.0), n=20))
+    solver.upload(q)
+    got = solver.observe(300.0, 0.6)
+    want = oracle.observe(op, g, fl, q, 300.0, 0.6)
+    for k in ("bulk", "elastic", "anchoring", "total", "radiality", "avg_S", "max_S"):
+        assert got[k] == pytest.approx(want[k], rel=1e-10, abs=1e-300), k
+    for k in ("radiality_count", "core_count", "defect_count", "defect_plaquettes", "xi_edges"):
+        assert got[k] == want[k], k
+    for k in ("defect_density", "xi_grad_proxy", "checker_rel"):
+        if math.isnan(want[k]):
+            assert math.isnan(got[k]), k
+        else:
+            assert got[k] == pytest.approx(want[k], rel=1e-9), k
+    assert got["nonfinite_cells"] == 0
+
+
+def test_nematic_matches_oracle(oracle):
+    op, solver, d = make_pair(Nx=16, Ny=12, Nz=20, L1=6e-12)
+    g, fl = oracle.geometry(op)
+    q = fp32(oracle.init(op, g, 0, 3, 0.5))
+    solver.upload(q)
+    got = solver.nematic()
+    want = oracle.nematic(q)
+    assert np.abs(got - want).max() < 1e-12
+
+
+def test_long_run_fp32_error_budget(oracle):
+    # 2000 explicit steps, L1 + strong anchoring, equilibrium shell order.
+    op, solver, d = make_pair(Nx=32, Ny=32, Nz=32, L1=6e-12, T_star=307.0)
+    g, fl = oracle.geometry(op)
+    T = 300.0
+    S_shell = S_eq(*bulk_ABC(d["a"], d["b"], d["c"], T, d["T_star"]))
+    q0 = fp32(oracle.init(op, g, 0, 42, 0.5))
+    dt = _dt(d, T)
+    solver.upload(q0)
+    solver.step(2000, T, S_shell, dt)
+    got = solver.download()
+    want = oracle.step_explicit(op, g, fl, q0, T, S_shell, dt, n=2000)
+    assert rel_err(got, want) <= 1e-5
+    assert rms_rel(got, want) <= 1e-6
+    eg = solver.observe(T, S_shell)["total"]
+    ew = oracle.observe(op, g, fl, want, T, S_shell)["total"]
+    assert eg == pytest.approx(ew, rel=1e-6)
+
+
+def test_noise_stream_matches_philox_box_muller(oracle):
+    # With Q = 0, A = 0 (T = T*) and no gradients the update is the noise alone, so the device
+    # noise can be read back and compared with Philox4x32-10 + Box-Muller evaluated here.
+    op, solver, d = make_pair(Nx=8, Ny=8, Nz=8, L1=6e-12, W=1e-5)
+    g, fl = oracle.geometry(op)
+    solver.upload(np.zeros(5 * 512))
+    sigma, seed, step = 1e-3, 0x1234ABCD5678EF01, 17
+    solver.step(1, d["T_star"], 0.0, 1e-12, noise_sigma=sigma, seed=seed, step_index=step)
+    got = solver.download().reshape(-1, 5)
+    move = (fl & 2) != 0  # evolving cells (ORC_EVOLVE with W > 0)
+    k0, k1 = seed & 0xFFFFFFFF, seed >> 32
+    idx = np.flatnonzero(move)
+    for cell in idx[:: max(1, len(idx) // 40)]:
+        z = []
+        for blk in range(2):
+            w = oracle.philox([int(cell), 0, step & 0xFFFFFFFF, ((step >> 32) << 1) | blk], [k0, k1])
+            for p in range(2):
+                u1 = ((w[2 * p] >> 8) + 1.0) / 16777216.0
+                u2 = ((w[2 * p + 1] >> 8) + 1.0) / 16777216.0
+                r = math.sqrt(-2.0 * math.log(u1))
+                z += [r * math.cos(2 * math.pi * u2), r * math.sin(2 * math.pi * u2)]
+        assert np.allclose(got[cell], sigma * np.array(z[:5]), rtol=2e-5, atol=1e-5 * sigma)
+    assert np.all(got[~move] == 0.0)
+    # distribution: zero mean, unit variance over all evolving cells and components
+    zs = got[move].ravel() / sigma
+    assert abs(zs.mean()) < 0.1 and abs(zs.var() - 1.0) < 0.15
+
+
+def test_step_rejects_bad_arguments(oracle):
+    from lcdrsimulator_b200 import LdgError
+    op, solver, d = make_pair(Nx=8, Ny=8, Nz=8)
+    with pytest.raises(LdgError, match="no field"):
+        solver.step(1, 300.0, 0.5, 1e-10)
+    solver.upload(np.zeros(5 * 512))
+    with pytest.raises(LdgError, match="dt"):
+        solver.step(1, 300.0, 0.5, -1.0)
+    with pytest.raises(LdgError, match="expected"):
+        solver.upload(np.zeros(10))
