@@ -266,8 +266,14 @@ def main():
     t_step = ms / 1e3 / args.steps
     value = world * box * args.steps / (ms / 1e3)
     touched = geo["active_cells"]
+    written = geo["written_cells"] if os.environ.get("LDG_QSR_KERNEL", "") != "direct" else box
+    if os.environ.get("LDG_QSR_KERNEL", "") == "direct":
+        touched = box
     peak, peak_kind = load_peaks()
-    achieved = BYTES_PER_CELL * touched / t_step / 1e9
+    # algorithmic bytes per launch: each visited cell's 5 FP32 components read once, each
+    # changing cell's 5 components written once
+    alg_bytes = (BYTES_PER_CELL // 2) * (touched + written)
+    achieved = alg_bytes / t_step / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "qsr_step_traffic.json")
     if os.path.exists(tfile):
@@ -328,7 +334,8 @@ def main():
                        "l2": "inputs larger than L2 (two 5-component FP32 fields of 335 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "bytes_per_cell_update": BYTES_PER_CELL, "kernel_ms": t_step * 1e3},
+                         "bytes_per_launch": alg_bytes, "read_cells": touched, "written_cells": written,
+                         "kernel_ms": t_step * 1e3},
             "clocks": clocks,
             "e2e": e2e,
             "gpu_launches": launches,

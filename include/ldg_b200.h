@@ -53,7 +53,8 @@ typedef struct qsr_geometry_info {
     double delta_eff;               /* shell volume / ellipsoid area (QSR.cu:174-185)         */
     long long shell_cells;          /* cells with |sd| <= shell_half_thickness                */
     long long evolving_cells;       /* cells the update touches                               */
-    long long active_cells;         /* cells in tiles the step kernel visits                  */
+    long long active_cells;         /* cells in tiles the step kernel visits (read per step)  */
+    long long written_cells;        /* cells the step writes (moving + strongly anchored)     */
     long long box_cells;            /* Nx*Ny*Nz                                               */
 } qsr_geometry_info;
 

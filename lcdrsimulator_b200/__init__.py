@@ -41,7 +41,7 @@ class QsrParams(C.Structure):
 class QsrGeometry(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("center_x", "center_y", "center_z", "radius_x", "radius_y",
                                           "radius_z", "min_spacing", "shell_half_thickness", "delta_eff")] + [
-        (n, C.c_longlong) for n in ("shell_cells", "evolving_cells", "active_cells", "box_cells")]
+        (n, C.c_longlong) for n in ("shell_cells", "evolving_cells", "active_cells", "written_cells", "box_cells")]
 
 
 class QsrStepArgs(C.Structure):

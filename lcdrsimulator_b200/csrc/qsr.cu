@@ -551,7 +551,7 @@ struct qsr_handle {
     qsr_params p{};
     Geometry g{};
     double delta_eff = 0.0;
-    long long shell_cells = 0, evolving_cells = 0, active_cells = 0;
+    long long shell_cells = 0, evolving_cells = 0, active_cells = 0, written_cells = 0;
     int sj = 0;
     long long si = 0, sc = 0, ncells = 0;
     float* q[2] = {nullptr, nullptr};
@@ -734,12 +734,13 @@ int qsr_create(const qsr_params* params, qsr_handle** out) {
         qsr_destroy(h);
         return LDG_ERR_CUDA;
     }
-    rc = tiled_plan_build(h->tiled, p.Nx, p.Ny, p.Nz, h->sj, h->si, fl.data());
+    rc = tiled_plan_build(h->tiled, p.Nx, p.Ny, p.Nz, h->sj, h->si, fl.data(), h->q[0], h->q[1], h->sc);
     if (rc != LDG_OK) {
         qsr_destroy(h);
         return rc;
     }
     h->active_cells = h->tiled.active_cells;
+    h->written_cells = h->tiled.written_cells;
     *out = h;
     return LDG_OK;
 }
@@ -755,6 +756,7 @@ int qsr_geometry(const qsr_handle* h, qsr_geometry_info* o) {
     o->shell_cells = h->shell_cells;
     o->evolving_cells = h->evolving_cells;
     o->active_cells = h->active_cells;
+    o->written_cells = h->written_cells;
     o->box_cells = h->ncells;
     return LDG_OK;
 }
@@ -848,7 +850,7 @@ int qsr_download(qsr_handle* h, double* q) {
     LDG_LAUNCHED("k_soa_to_aos");
     LDG_CUDA(cudaMemcpyAsync(q, h->stage, (size_t)h->ncells * 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     LDG_CUDA(cudaStreamSynchronize(h->stream));
-    return LDG_OK;
+    return tiled_check(h->tiled, h->stream);
 }
 
 int qsr_nematic(qsr_handle* h, double* s_n) {
@@ -901,7 +903,7 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
         float* outb = h->q[1 - h->cur];
         if (!imex) {
             if (choice == 1 && h->tiled.ok) {
-                int rc = tiled_step(h->tiled, in, outb, h->flags, P, L2, L3, noise, h->stream);
+                int rc = tiled_step(h->tiled, in, outb, h->flags, P, L2, L3, noise, false, h->stream);
                 if (rc) return rc;
             } else {
                 dispatch_direct<false>(h, in, outb, P, L2, L3, noise);
@@ -910,7 +912,12 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             LDG_LAUNCHED("qsr step kernel");
             h->cur = 1 - h->cur;
         } else {
-            dispatch_direct<true>(h, in, h->rhs, P, L2, L3, noise);
+            if (choice == 1 && h->tiled.ok) {
+                int rc = tiled_step(h->tiled, in, h->rhs, h->flags, P, L2, L3, noise, true, h->stream);
+                if (rc) return rc;
+            } else {
+                dispatch_direct<true>(h, in, h->rhs, P, L2, L3, noise);
+            }
             h->launches++;
             LDG_LAUNCHED("k_step_direct(rhs)");
             dim3 blk(32, 8, 1), grd((p.Nz + 31) / 32, (p.Ny + 7) / 8, p.Nx);
@@ -990,6 +997,10 @@ int qsr_observe(qsr_handle* h, const qsr_observe_args* a, qsr_observables* o) {
     LDG_CUDA(cudaMemcpyAsync(&R, h->opart + kObsBlocks, sizeof(R), cudaMemcpyDeviceToHost, h->stream));
     if (wd || wx) LDG_CUDA(cudaMemcpyAsync(&SR, h->spart + kSliceBlocks, sizeof(SR), cudaMemcpyDeviceToHost, h->stream));
     LDG_CUDA(cudaStreamSynchronize(h->stream));
+    {
+        const int rc = tiled_check(h->tiled, h->stream);
+        if (rc) return rc;
+    }
     const double nan = std::numeric_limits<double>::quiet_NaN();
     std::memset(o, 0, sizeof(*o));
     o->bulk = R.bulk; o->elastic = R.elastic; o->anchoring = R.anch;
@@ -1021,7 +1032,7 @@ int qsr_sync(qsr_handle* h) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "qsr_sync: null handle");
     LDG_CUDA(cudaStreamSynchronize(h->stream));
-    return LDG_OK;
+    return tiled_check(h->tiled, h->stream);
 }
 
 void* qsr_stream(qsr_handle* h) { return h ? (void*)h->stream : nullptr; }

@@ -1,31 +1,433 @@
-// Launch plan of the tiled confined-solver step kernel. The plan records which tiles of
-// the box contain cells the step must visit; tiles that hold only frozen exterior cells are
-// skipped (their values never change and are identical in both ping-pong buffers).
+// Tiled confined-solver step kernel for sm_100a.
+//
+// A CTA owns a (TJ x TK) column tile of the (j, k) plane and marches along i over a chunk
+// of planes. Each plane of the input field arrives in shared memory through one TMA load
+// of a 4-D box (k, j, i, component) covering the tile plus a halo of 2 rows and 4 columns
+// (the k start stays on a 16-byte boundary), so every Q value is read from HBM about once.
+// The ring holds the planes i-2 .. i+2 plus PF planes in flight. The column divergence D
+// (needed by the L2 and L3 terms) is computed once per plane on the tile plus a 1-cell halo
+// into a 3-plane shared ring. Per cell the kernel then evaluates the chemical potential and
+// the update from shared memory and writes only the cells that change (moving and strongly
+// anchored cells): frozen exterior cells hold identical values in both ping-pong buffers.
+// Tiles that contain no changing cell are never visited (host-built work list).
+//
+// mbarrier waits are bounded: on timeout the kernel records LDG_ERR_TIMEOUT in a device
+// word, waits (bounded) for its own TMA loads and returns.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "ldg_api_common.h"
 #include "ldg_common.cuh"
 
 namespace ldg {
 
-struct TiledPlan {
-    bool ok = false;
-    long long active_cells = 0;
+namespace tiled {
+
+constexpr int TK = 32;               // tile width along k (one warp per row)
+constexpr int TJ = 8;                // tile rows along j (one warp each)
+constexpr int THREADS = TK * TJ;
+constexpr int HJ = 2, HK = 4;        // halo rows / columns loaded with each plane
+constexpr int RW = TK + 2 * HK;      // 40 floats per smem row
+constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
+constexpr int CSTR = RW * ROWS;      // floats per component plane
+constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
+constexpr int PF = 2;                // planes in flight beyond i+2
+constexpr int NQ = 5 + PF;           // ring slots
+constexpr int DRW = TK + 2, DROWS = TJ + 2;
+constexpr int DCSTR = DRW * DROWS;
+constexpr int DPLANE = 3 * DCSTR;
+constexpr uint32_t PLANE_BYTES = PLANE * 4;
+constexpr int CHUNK = 32;            // planes per work item
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase with the given parity, giving up after WAIT_NS of wall time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity) {
+    if (mbar_try_wait(b, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(b, parity)) return true;
+        if (global_ns() - t0 > WAIT_NS) return false;
+    }
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(su32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(su32(bar))
+        : "memory");
+}
+
+// Shared-memory Q accessor centred on local cell (jl, kl) of plane i; planes i-2..i+2.
+struct SmemQ {
+    const float* pl[5];
+    int off;
+    __device__ __forceinline__ float operator()(int c, int di, int dj, int dk) const {
+        const float* s = pl[di + 2] + off + dj * RW + dk;
+        if (c < 5) return s[c * CSTR];
+        return -(s[0] + s[3 * CSTR]);
+    }
 };
 
-inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int, long long, const uint8_t*) {
-    plan.ok = false;
-    plan.active_cells = (long long)Nx * Ny * Nz;
-    return 0;
+// Shared-memory D accessor centred on local cell (jl, kl) of plane i; planes i-1..i+1.
+struct SmemD {
+    const float* pl[3];
+    int off;
+    __device__ __forceinline__ float operator()(int comp, int di, int dj, int dk) const {
+        return pl[di + 1][off + comp * DCSTR + dj * DRW + dk];
+    }
+};
+
+template <bool kL2, bool kL3, bool kNoise, bool kRHS>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
+                 const int4* __restrict__ items, QsrConst P, int* __restrict__ err) {
+    constexpr bool kD = kL2 || kL3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* sq = reinterpret_cast<float*>(smem_raw);
+    float* sd = sq + NQ * PLANE;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sd + (kD ? 3 * DPLANE : 0));
+    int* s_abort = reinterpret_cast<int*>(bar + NQ);
+
+    const int4 item = items[blockIdx.x];
+    const int j0 = item.x, k0 = item.y, ib = item.z, ie = item.w;
+    const int base = ib - 2;  // first plane this CTA loads; slots and phases count from it
+    const int tid = threadIdx.x;
+    const int kl = tid & (TK - 1), jl = tid / TK;
+
+    // Plane p (p >= base) lives in slot (p - base) % NQ; its load completes that slot's
+    // barrier phase number (p - base) / NQ.
+    auto slot = [&](int p) { return (p - base) % NQ; };
+    auto parity = [&](int p) { return (uint32_t)(((p - base) / NQ) & 1); };
+
+    if (tid == 0) {
+        for (int s = 0; s < NQ; ++s) mbar_init(&bar[s], 1);
+        mbar_fence_init();
+        *s_abort = 0;
+    }
+    __syncthreads();
+
+    // Planes outside the grid complete their phase with a plain arrive (no data).
+    auto issue = [&](int p) {
+        uint64_t* b = &bar[slot(p)];
+        if (p >= 0 && p < P.Nx) {
+            mbar_expect_tx(b, PLANE_BYTES);
+            tma_load_4d(sq + slot(p) * PLANE, &tm_in, k0 - HK, j0 - HJ, p, 0, b);
+        } else {
+            mbar_arrive(b);
+        }
+    };
+    int issued_end = base + NQ;  // planes [base, issued_end) have been issued (tracked by every thread)
+    if (tid == 0) {
+        fence_proxy_async();
+        for (int p = base; p < base + NQ; ++p) issue(p);
+    }
+    int waited_end = base;       // planes [base, waited_end) have been waited for
+    auto wait_plane = [&](int p) {
+        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
+            atomicExch(err, LDG_ERR_TIMEOUT);
+            *s_abort = 1;
+        }
+        waited_end = p + 1;
+    };
+
+    // Column divergence of plane p on the tile plus a 1-cell halo into D slot (p + 1) % 3.
+    // Reads Q planes p-1 .. p+1 (all waited for by the caller).
+    auto compute_D = [&](int p) {
+        if (p < 0 || p >= P.Nx) return;
+        float* dst = sd + ((p + 1) % 3) * DPLANE;
+        SmemQ A;
+#pragma unroll
+        for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(p + d - 2, base)) * PLANE;
+        for (int t = tid; t < DROWS * DRW; t += THREADS) {
+            const int r = t / DRW, cidx = t - r * DRW;
+            const int j = j0 + r - 1, k = k0 + cidx - 1;
+            float D[3] = {0.0f, 0.0f, 0.0f};
+            if (j >= 0 && j < P.Ny && k >= 0 && k < P.Nz) {
+                A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
+                dcol_at(A, P, p, j, k, 0, 0, 0, D);
+            }
+            dst[t] = D[0];
+            dst[DCSTR + t] = D[1];
+            dst[2 * DCSTR + t] = D[2];
+        }
+    };
+
+    // Prologue: planes ib-2 .. ib+1, then D(ib-1) and D(ib).
+    for (int p = base; p <= ib + 1; ++p) wait_plane(p);
+    __syncthreads();
+    if (kD && !*s_abort) {
+        compute_D(ib - 1);
+        compute_D(ib);
+    }
+
+    const int j = j0 + jl, k = k0 + kl;
+    const bool in_grid = (j < P.Ny) && (k < P.Nz);
+    for (int i = ib; i < ie; ++i) {
+        wait_plane(i + 2);
+        __syncthreads();
+        if (*s_abort) break;
+        if (kD) {
+            compute_D(i + 1);
+            __syncthreads();
+        }
+        if (in_grid) {
+            const long long id = (long long)i * P.si + (long long)j * P.sj + k;
+            const uint8_t f = __ldg(flags + id);
+            const bool fixed = !kRHS && (f & kFixed);
+            const bool move = (f & kMove) != 0;
+            if (fixed || move) {
+                SmemQ A;
+#pragma unroll
+                for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(i + d - 2, base)) * PLANE;
+                A.off = (jl + HJ) * RW + (kl + HK);
+                float c[5], o[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) c[m] = A(m, 0, 0, 0);
+                if (fixed) {
+                    surface_q0(P, i, j, k, o);
+                } else {
+                    SmemD DA;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) DA.pl[d] = sd + ((i + d) % 3) * DPLANE;
+                    DA.off = (jl + 1) * DRW + (kl + 1);
+                    float mu[5], lap[5];
+                    chem_potential<kL2, kL3>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                    const uint32_t cell = (uint32_t)(k + P.Nz * (j + P.Ny * i));
+                    if (kRHS) {
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) o[m] = c[m] - P.mob_dt * mu[m] - P.alpha * lap[m];
+                        if (kNoise) {
+                            float g[5];
+                            normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+                            for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
+                        }
+                    } else {
+                        euler_update(P, c, mu, cell, kNoise, o);
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
+            }
+        }
+        __syncthreads();
+        // Plane i-2 is dead: its slot takes plane i-2+NQ.
+        if (tid == 0) {
+            fence_proxy_async();
+            issue(issued_end);
+        }
+        ++issued_end;
+    }
+    // Drain: every load this CTA issued lands before its shared memory is released.
+    for (int p = waited_end; p < issued_end; ++p) {
+        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) atomicExch(err, LDG_ERR_TIMEOUT);
+    }
 }
 
-inline int tiled_step(const TiledPlan&, const float*, float*, const uint8_t*, const QsrConst&, bool, bool, bool,
-                      cudaStream_t) {
-    return 0;
+}  // namespace tiled
+
+struct TiledPlan {
+    bool ok = false;
+    long long active_cells = 0;   // cells inside visited tiles (each read once per step)
+    long long written_cells = 0;  // cells written per step (moving + strongly anchored)
+    int n_items = 0;
+    int4* items = nullptr;        // device work list (j0, k0, i_begin, i_end)
+    int* err = nullptr;           // device error word
+    CUtensorMap tmap[2];
+    const float* bufs[2] = {nullptr, nullptr};
+    size_t smem_bytes[2] = {0, 0};  // [no D, with D]
+};
+
+inline int tiled_encode(CUtensorMap* tm, const float* base, int Nx, int Ny, int Nz, int sj, long long si, long long sc) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled entry point unavailable");
+            return LDG_ERR_CUDA;
+        }
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t dims[4] = {(cuuint64_t)Nz, (cuuint64_t)Ny, (cuuint64_t)Nx, 5};
+    cuuint64_t strides[3] = {(cuuint64_t)sj * 4, (cuuint64_t)si * 4, (cuuint64_t)sc * 4};
+    cuuint32_t box[4] = {tiled::RW, tiled::ROWS, 1, 5};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void*)base, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+        return LDG_ERR_CUDA;
+    }
+    return LDG_OK;
 }
 
-inline void tiled_plan_free(TiledPlan& plan) { plan = TiledPlan{}; }
+// Builds the work list from the host classification and encodes the two tensor maps.
+inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, long long si, const uint8_t* fl,
+                            const float* buf0, const float* buf1, long long sc) {
+    using namespace tiled;
+    plan = TiledPlan{};
+    const int ntj = (Ny + TJ - 1) / TJ, ntk = (Nz + TK - 1) / TK;
+    std::vector<int4> items;
+    long long active = 0, written = 0;
+    for (int jt = 0; jt < ntj; ++jt)
+        for (int kt = 0; kt < ntk; ++kt) {
+            int imin = Nx, imax = -1;
+            for (int i = 0; i < Nx; ++i) {
+                bool any = false;
+                for (int j = jt * TJ; j < std::min(Ny, (jt + 1) * TJ) && !any; ++j)
+                    for (int k = kt * TK; k < std::min(Nz, (kt + 1) * TK); ++k) {
+                        const uint8_t f = fl[(size_t)i * si + (size_t)j * sj + k];
+                        if (f & (kMove | kFixed)) {
+                            any = true;
+                            ++written;
+                        }
+                    }
+                if (any) { imin = std::min(imin, i); imax = std::max(imax, i); }
+            }
+            if (imax < 0) continue;
+            const long long tile_cells = (long long)(std::min(Ny, (jt + 1) * TJ) - jt * TJ) *
+                                         (std::min(Nz, (kt + 1) * TK) - kt * TK);
+            active += tile_cells * (imax - imin + 1);
+            for (int i = imin; i <= imax; i += CHUNK)
+                items.push_back(make_int4(jt * TJ, kt * TK, i, std::min(imax + 1, i + CHUNK)));
+        }
+    // `written` above counts cells per (row) once a row has one; recount exactly.
+    written = 0;
+    for (int i = 0; i < Nx; ++i)
+        for (int j = 0; j < Ny; ++j)
+            for (int k = 0; k < Nz; ++k)
+                if (fl[(size_t)i * si + (size_t)j * sj + k] & (kMove | kFixed)) ++written;
+    // Launch order: plane chunk slowest, so CTAs resident together cover neighbouring tiles of
+    // the same planes and their halo rows are served from L2.
+    std::stable_sort(items.begin(), items.end(), [](const int4& a, const int4& b) {
+        if (a.z != b.z) return a.z < b.z;
+        if (a.x != b.x) return a.x < b.x;
+        return a.y < b.y;
+    });
+    plan.active_cells = active;
+    plan.written_cells = written;
+    plan.n_items = (int)items.size();
+    if (plan.n_items > 0) {
+        LDG_CUDA(cudaMalloc(&plan.items, items.size() * sizeof(int4)));
+        LDG_CUDA(cudaMemcpy(plan.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    LDG_CUDA(cudaMalloc(&plan.err, sizeof(int)));
+    LDG_CUDA(cudaMemset(plan.err, 0, sizeof(int)));
+    int rc = tiled_encode(&plan.tmap[0], buf0, Nx, Ny, Nz, sj, si, sc);
+    if (rc) return rc;
+    rc = tiled_encode(&plan.tmap[1], buf1, Nx, Ny, Nz, sj, si, sc);
+    if (rc) return rc;
+    plan.bufs[0] = buf0;
+    plan.bufs[1] = buf1;
+    plan.smem_bytes[0] = (size_t)NQ * PLANE * 4 + NQ * 8 + 16;
+    plan.smem_bytes[1] = (size_t)NQ * PLANE * 4 + (size_t)3 * DPLANE * 4 + NQ * 8 + 16;
+    plan.ok = true;
+    return LDG_OK;
+}
+
+template <bool L2, bool L3, bool N, bool R>
+inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const uint8_t* flags, const QsrConst& P,
+                          cudaStream_t st) {
+    using namespace tiled;
+    constexpr bool kD = L2 || L3;
+    const size_t smem = plan.smem_bytes[kD ? 1 : 0];
+    static bool configured = false;
+    if (!configured) {
+        LDG_CUDA(cudaFuncSetAttribute(k_step_tiled<L2, L3, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    if (plan.n_items == 0) return LDG_OK;
+    k_step_tiled<L2, L3, N, R><<<plan.n_items, THREADS, smem, st>>>(plan.tmap[which], out, flags, plan.items, P,
+                                                                    plan.err);
+    return LDG_OK;
+}
+
+// One step through the tiled kernel. `in` must be one of the two planned buffers.
+inline int tiled_step(const TiledPlan& plan, const float* in, float* out, const uint8_t* flags, const QsrConst& P,
+                      bool L2, bool L3, bool noise, bool rhs, cudaStream_t st) {
+    const int which = (in == plan.bufs[0]) ? 0 : 1;
+    const int key = (L2 ? 1 : 0) | (L3 ? 2 : 0) | (noise ? 4 : 0);
+    if (!rhs) {
+        switch (key) {
+            case 0: return tiled_launch_t<false, false, false, false>(plan, which, out, flags, P, st);
+            case 1: return tiled_launch_t<true, false, false, false>(plan, which, out, flags, P, st);
+            case 2: return tiled_launch_t<false, true, false, false>(plan, which, out, flags, P, st);
+            case 3: return tiled_launch_t<true, true, false, false>(plan, which, out, flags, P, st);
+            case 4: return tiled_launch_t<false, false, true, false>(plan, which, out, flags, P, st);
+            case 5: return tiled_launch_t<true, false, true, false>(plan, which, out, flags, P, st);
+            case 6: return tiled_launch_t<false, true, true, false>(plan, which, out, flags, P, st);
+            default: return tiled_launch_t<true, true, true, false>(plan, which, out, flags, P, st);
+        }
+    }
+    switch (key) {
+        case 0: return tiled_launch_t<false, false, false, true>(plan, which, out, flags, P, st);
+        case 1: return tiled_launch_t<true, false, false, true>(plan, which, out, flags, P, st);
+        case 2: return tiled_launch_t<false, true, false, true>(plan, which, out, flags, P, st);
+        case 3: return tiled_launch_t<true, true, false, true>(plan, which, out, flags, P, st);
+        case 4: return tiled_launch_t<false, false, true, true>(plan, which, out, flags, P, st);
+        case 5: return tiled_launch_t<true, false, true, true>(plan, which, out, flags, P, st);
+        case 6: return tiled_launch_t<false, true, true, true>(plan, which, out, flags, P, st);
+        default: return tiled_launch_t<true, true, true, true>(plan, which, out, flags, P, st);
+    }
+}
+
+// Reads and clears the device error word (LDG_OK when no bounded wait gave up).
+inline int tiled_check(const TiledPlan& plan, cudaStream_t st) {
+    if (!plan.err) return LDG_OK;
+    int e = 0;
+    LDG_CUDA(cudaMemcpyAsync(&e, plan.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LDG_CUDA(cudaStreamSynchronize(st));
+    if (e != 0) {
+        LDG_CUDA(cudaMemsetAsync(plan.err, 0, sizeof(int), st));
+        set_error("tiled step: a bounded shared-memory pipeline wait gave up");
+        return LDG_ERR_TIMEOUT;
+    }
+    return LDG_OK;
+}
+
+inline void tiled_plan_free(TiledPlan& plan) {
+    cudaFree(plan.items);
+    cudaFree(plan.err);
+    plan = TiledPlan{};
+}
 
 }  // namespace ldg

@@ -1,0 +1,719 @@
+// qsr_b200 -- drop-in host program for `QSR_cuda --config <file>` (the reference's QSR.cu main).
+//
+// Same key=value configuration keys and defaults, same simulation modes (1 single temperature,
+// 2 temperature sweep, 3 quench), same guards and exit codes, same log headers and number
+// formatting, same field writers. Every device operation goes through the C ABI in
+// include/ldg_b200.h. Interactive prompting is not provided: the program runs from --config.
+//
+// Keys added on top of the reference (all optional, reference behaviour when absent):
+//   droplet_radius_cells       droplet radius in cells (centre stays at (N-1)/2)
+//   noise_strength             quench Langevin noise, sigma^2 = 2 (1/gamma) noise_strength dt
+//   noise_seed                 Philox key of the noise (default: random_seed, or 0)
+//   init_file                  warm start from a Qtensor_output_*.dat file (overrides init_mode)
+//   write_iteration_snapshots  single-T per-print nematic dumps (default y, as the reference)
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <filesystem>
+#include <iostream>
+#include <limits>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "host_common.hpp"
+#include "ldg_b200.h"
+
+namespace fs = std::filesystem;
+using namespace host;
+
+namespace {
+
+const double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+struct Fail {
+    std::string msg;
+};
+
+void check(int rc, const char* what) {
+    if (rc != LDG_OK) throw Fail{std::string(what) + " failed: " + ldg_last_error()};
+}
+
+struct DtResult {
+    double min_dx, S_scale, L_eff_total, D_total, dt_diff_total, L_eff_explicit, dt_diff, bulk_rate, dt_bulk, dt_max;
+    bool semi_implicit_active;
+};
+
+// estimate_stable_dt_window (QSR.cu:1528-1604).
+DtResult estimate_dt(double dx, double dy, double dz, double gamma, double a, double b, double c, double Ts,
+                     int mode, double kappa, double L1, double L2, double L3, double S_ref_used, double S0, double Ta,
+                     double Tb, bool semi, double L_stab, int jacobi) {
+    DtResult o{};
+    o.min_dx = std::min({dx, dy, dz});
+    o.S_scale = std::isfinite(S_ref_used) ? std::abs(S_ref_used) : std::max(std::abs(S0), 0.5);
+    const double sa = std::abs(equilibrium_shell_order(a, b, c, Ta, Ts, mode));
+    const double sb = std::abs(equilibrium_shell_order(a, b, c, Tb, Ts, mode));
+    if (std::isfinite(sa) && sa > 0.0) o.S_scale = std::max(o.S_scale, sa);
+    if (std::isfinite(sb) && sb > 0.0) o.S_scale = std::max(o.S_scale, sb);
+    o.S_scale = std::max(o.S_scale, 1.0);
+    const bool ldg = (L1 != 0.0 || L2 != 0.0 || L3 != 0.0);
+    const bool aniso = (L2 != 0.0 || L3 != 0.0);
+    o.L_eff_total = ldg ? std::max({std::abs(L1), std::abs(L2), std::abs(L1 + L2), std::abs(L1 + 2.0 * L2),
+                                    std::abs(L3) * o.S_scale})
+                        : std::abs(kappa);
+    if (!(o.L_eff_total > 0.0)) o.L_eff_total = 1e-12;
+    o.D_total = o.L_eff_total / gamma;
+    if (!(o.D_total > 0.0) || !std::isfinite(o.D_total)) o.D_total = 1e-12;
+    o.dt_diff_total = 0.5 * (o.min_dx * o.min_dx) / (6.0 * o.D_total);
+    if (aniso) o.dt_diff_total *= 0.25;
+    o.L_eff_explicit = o.L_eff_total;
+    o.dt_diff = o.dt_diff_total;
+    if (semi && L_stab > 0.0 && jacobi > 0) {
+        const double L_base = ldg ? L1 : kappa;
+        const double Ls = (L_base >= 0.0) ? L_stab : -L_stab;
+        const double L_rem = std::abs(L_base - Ls);
+        o.L_eff_explicit = ldg ? std::max({L_rem, std::abs(L2), std::abs(L1 + L2), std::abs(L1 + 2.0 * L2),
+                                           std::abs(L3) * o.S_scale})
+                               : L_rem;
+        if (o.L_eff_explicit > 0.0) {
+            o.dt_diff = 0.5 * (o.min_dx * o.min_dx) / (6.0 * (o.L_eff_explicit / gamma));
+            if (aniso) o.dt_diff *= 0.25;
+        } else {
+            o.dt_diff = std::numeric_limits<double>::infinity();
+        }
+        o.semi_implicit_active = true;
+    }
+    auto rate = [&](double T) {
+        double A, B, C;
+        bulk_ABC(a, b, c, T, Ts, mode, A, B, C);
+        return std::abs(A) + std::abs(B) * o.S_scale + std::abs(C) * o.S_scale * o.S_scale;
+    };
+    o.bulk_rate = std::max(rate(Ta), rate(Tb));
+    o.dt_bulk = (o.bulk_rate > 0.0) ? (0.02 * gamma / o.bulk_rate) : std::numeric_limits<double>::infinity();
+    o.dt_max = std::min(o.dt_diff, o.dt_bulk);
+    if (!(o.dt_max > 0.0) || !std::isfinite(o.dt_max)) o.dt_max = o.dt_diff;
+    return o;
+}
+
+void print_dt(const DtResult& e) {
+    std::cout << "\nMaximum stable dt estimates:\n"
+              << "  dt_diff (elastic) ~= " << e.dt_diff << " s\n"
+              << "  dt_diff_total     ~= " << e.dt_diff_total << " s"
+              << (e.semi_implicit_active ? " (before semi-implicit)" : "") << "\n"
+              << "  dt_bulk (bulk)    ~= " << e.dt_bulk << " s\n"
+              << "  dt_max            = " << e.dt_max << " s" << std::endl;
+}
+
+// correlation_length_guard (QSR.cu:1687-1800): returns false when xi is under-resolved.
+bool xi_guard(double dxs, double dys, double dzs, double rx, double ry, double rz, double a, double b, double c,
+              double T, double Ts, int mode, double kappa, double L1, double L2, double L3, bool enabled) {
+    const double min_d = std::min({dxs, dys, dzs});
+    double A, B, C;
+    bulk_ABC(a, b, c, T, Ts, mode, A, B, C);
+    const double absA_lin = std::abs(A);
+    const double Seq = S_eq(A, B, C);
+    const double fpp = (Seq > 0.0) ? (2.0 * A / 3.0 - (4.0 * B / 9.0) * Seq + (4.0 * C / 3.0) * Seq * Seq) : kNaN;
+    const double absA_nem = std::isfinite(fpp) ? std::abs(fpp) : kNaN;
+    const bool ldg = (L1 != 0.0 || L2 != 0.0 || L3 != 0.0);
+    double bmin, bmax, nmin, nmax, l3env = 0.0;
+    if (!ldg) {
+        bmin = bmax = nmin = nmax = std::abs(kappa);
+    } else {
+        bool have = false;
+        double lo = 0.0, hi = 0.0;
+        for (double v : {L1, L1 + L2, L1 + 2.0 * L2}) {
+            if (!std::isfinite(v) || !(v > 0.0)) continue;
+            if (!have) { lo = hi = v; have = true; }
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+        }
+        if (!have) {
+            const double fb = std::max({std::abs(L1), std::abs(L1 + L2), std::abs(L1 + 2.0 * L2), 1e-12});
+            bmin = bmax = nmin = nmax = fb;
+        } else {
+            bmin = lo; bmax = hi;
+            l3env = (Seq > 0.0 && std::isfinite(Seq)) ? std::abs(L3) * Seq : 0.0;
+            nmin = bmin; nmax = bmax;
+            if (l3env > 0.0) { nmin = std::max(bmin - l3env, 1e-12); nmax = bmax + l3env; }
+        }
+    }
+    auto xi = [](double L, double absA) { return (L <= 0.0 || absA <= 0.0) ? kNaN : std::sqrt(L / absA); };
+    const double xlmin = xi(bmin, absA_lin), xlmax = xi(bmax, absA_lin);
+    const double xnmin = xi(nmin, absA_nem), xnmax = xi(nmax, absA_nem);
+    const double xg = std::isfinite(xnmin) ? xnmin : xlmin;
+    const double xc = std::isfinite(xnmax) ? xnmax : (std::isfinite(xlmax) ? xlmax : xg);
+    const double rxr = (std::isfinite(xg) && dxs > 0.0) ? xg / dxs : 0.0;
+    const double ryr = (std::isfinite(xg) && dys > 0.0) ? xg / dys : 0.0;
+    const double rzr = (std::isfinite(xg) && dzs > 0.0) ? xg / dzs : 0.0;
+    const double worst = std::min({rxr, ryr, rzr});
+    std::cout << "\n--- Correlation Length (xi) Estimate ---\n";
+    if (std::isfinite(xg)) {
+        std::cout << "xi_guard = " << xg << " m, xi/dx = " << rxr << ", xi/dy = " << ryr << ", xi/dz = " << rzr
+                  << " (worst axis ratio = " << worst << ")\n";
+        std::cout << "Best-axis ratio xi/min(dx,dy,dz) = " << ((min_d > 0.0) ? xg / min_d : 0.0) << "\n";
+        const double mr = std::min({xc > 0 ? rx / xc : 0.0, xc > 0 ? ry / xc : 0.0, xc > 0 ? rz / xc : 0.0});
+        std::cout << "Geometry confinement ratio min(R/xi_conf) = " << mr << "\n";
+    } else {
+        std::cout << "xi estimate unavailable (check elastic stiffness and that T is not exactly T*)\n";
+    }
+    if (!enabled) return true;
+    if (std::isfinite(xg) && worst < 2.0) {
+        std::cout << "\n[WARN] xi is under-resolved on the coarsest grid axis (worst xi/dh ≈ " << worst << " < 2).\n";
+        std::cout << "       Non-interactive run: aborting instead of prompting.\n";
+        return false;
+    }
+    return true;
+}
+
+struct Run {
+    Config cfg;
+    qsr_handle* h = nullptr;
+    qsr_params p{};
+    int Nx = 0, Ny = 0, Nz = 0;
+    long long n = 0;
+    ~Run() {
+        if (h) qsr_destroy(h);
+    }
+};
+
+qsr_observables observe(Run& r, double T, double S_shell, int dz, double dthr, double dcut, int xz, double xthr,
+                        bool want_def, bool want_xi) {
+    qsr_observe_args a{T, S_shell, dz, dthr, dcut, xz, xthr, want_def ? 1 : 0, want_xi ? 1 : 0};
+    qsr_observables o{};
+    check(qsr_observe(r.h, &a, &o), "qsr_observe");
+    return o;
+}
+
+std::vector<double> nematic(Run& r) {
+    std::vector<double> s((size_t)(4 * r.n));
+    check(qsr_nematic(r.h, s.data()), "qsr_nematic");
+    return s;
+}
+
+std::vector<double> download(Run& r) {
+    std::vector<double> q((size_t)(5 * r.n));
+    check(qsr_download(r.h, q.data()), "qsr_download");
+    return q;
+}
+
+void print_help() {
+    std::cout << "qsr_b200 options:\n"
+              << "  --config <path>       Run non-interactively using key=value config file\n"
+              << "  --dry-run             Resolve the configuration and print it; no GPU work\n"
+              << "  --help                Show this help\n";
+}
+
+int run_main(int argc, char** argv) {
+    std::string config_path;
+    bool dry = false;
+    for (int i = 1; i < argc; ++i) {
+        const std::string arg = argv[i] ? argv[i] : "";
+        if (arg == "--help" || arg == "-h") { print_help(); return 0; }
+        if (arg == "--config" && i + 1 < argc) { config_path = argv[++i]; continue; }
+        if (arg == "--dry-run") { dry = true; continue; }
+        if (arg == "--interactive") {
+            std::cerr << "qsr_b200: interactive prompting is not provided; use --config" << std::endl;
+            return 2;
+        }
+    }
+    if (config_path.empty()) {
+        std::cerr << "qsr_b200: --config <path> is required (see --help)" << std::endl;
+        return 2;
+    }
+    Run R;
+    Config& cfg = R.cfg;
+    parse_config(config_path, cfg, false);
+    std::cout << "\033[1mQ-tensor evolution simulation (B200)\033[0m\n" << std::endl;
+    std::cout << "[Config] Running non-interactively with " << config_path << "\n";
+
+    int mode = get<int>(cfg, "init_mode", 1);
+    mode = std::min(std::max(mode, 0), 2);
+    const long long random_seed = get<long long>(cfg, "random_seed", -1);
+    const int Nx = get<int>(cfg, "Nx", 100), Ny = get<int>(cfg, "Ny", 100), Nz = get<int>(cfg, "Nz", 100);
+    const double dx = get<double>(cfg, "dx", 1e-8), dy = get<double>(cfg, "dy", 1e-8), dz = get<double>(cfg, "dz", 1e-8);
+    const double a = get<double>(cfg, "a", 0.044e6), b = get<double>(cfg, "b", 1.413e6), c = get<double>(cfg, "c", 1.153e6);
+    const double T = get<double>(cfg, "T", 300.0), T_star = get<double>(cfg, "T_star", 308.0);
+    const int modechoice = get<int>(cfg, "bulk_modechoice", 1);
+    double A, B, C;
+    bulk_ABC(a, b, c, T, T_star, modechoice, A, B, C);
+    const double Seq = S_eq(A, B, C);
+    std::cout << "\nBulk convention: " << (modechoice == 1 ? "std" : "ravnik") << "\nComputed S_c (heuristic) = "
+              << b / (2.0 * c) << ", S_eq(T=" << T << "K) = " << Seq << std::endl;
+    const double S0 = get<double>(cfg, "S0", Seq > 0 ? Seq : 0.5);
+    double kappa = get<double>(cfg, "kappa", 6.5e-12);
+    const bool frank = get<bool>(cfg, "use_frank_map", false);
+    double L1 = 0.0, L2 = 0.0, L3 = 0.0, S_ref_used = kNaN;
+    if (frank) {
+        // Frank -> LdG mapping (QSR.cu:2004-2056).
+        const double K1 = get<double>(cfg, "K1", 6.5e-12), K2 = get<double>(cfg, "K2", 4.0e-12);
+        const double K3 = get<double>(cfg, "K3", 8e-12);
+        double S_ref = get<double>(cfg, "S_ref", (Seq > 0.0) ? Seq : ((S0 > 0.0) ? S0 : (b / (2.0 * c))));
+        if (S_ref <= 1e-12) S_ref = 0.5;
+        S_ref_used = S_ref;
+        const double S2 = S_ref * S_ref, S3 = S2 * S_ref;
+        L2 = (K1 - K2) / S2;
+        L3 = (9.0 / 4.0) * (K3 - K1) / S3;
+        L1 = (K1 + K2 - K3) / (2.0 * S2);
+        kappa = 0.0;
+        std::cout << "Mapped L1=" << L1 << ", L2=" << L2 << ", L3=" << L3 << " (Q=S(nn-I/3), S_ref=" << S_ref
+                  << ", Kappa set to 0)" << std::endl;
+        if (!(L1 > 0.0) || !((L1 + L2) > 0.0)) {
+            std::cout << "\n[WARNING] Potentially unstable elastic parameters (L1=" << L1 << ", L2=" << L2
+                      << ", L1+L2=" << (L1 + L2) << ").\n";
+            if (!get<bool>(cfg, "proceed_unstable_elastic", false)) {
+                std::cout << "Aborting this run; choose different K1/K2/K3 or do not use Frank mapping." << std::endl;
+                return 1;
+            }
+        }
+    } else {
+        L1 = get<double>(cfg, "L1", 0.0);
+        L2 = get<double>(cfg, "L2", 0.0);
+        L3 = get<double>(cfg, "L3", 0.0);
+        if (L1 != 0 || L2 != 0 || L3 != 0) kappa = 0.0;
+        if ((L1 != 0.0 || L2 != 0.0) && (!(L1 > 0.0) || !((L1 + L2) > 0.0))) {
+            std::cout << "\n[ERROR] Unstable elastic parameters for this model (L1=" << L1 << ", L2=" << L2
+                      << ", L1+L2=" << (L1 + L2) << ").\n";
+            if (!get<bool>(cfg, "proceed_unstable_elastic", false)) {
+                std::cout << "Aborting this run; choose stable L1/L2 or use kappa instead." << std::endl;
+                return 1;
+            }
+        }
+    }
+    const double radius_cells = get<double>(cfg, "droplet_radius_cells", 0.0);
+    double ridx = 0.5 * ((double)std::min({Nx, Ny, Nz}) - 1.0);
+    if (radius_cells > 0.0) ridx = radius_cells;
+    const double rx = std::max(ridx * dx, 0.5 * dx), ry = std::max(ridx * dy, 0.5 * dy), rz = std::max(ridx * dz, 0.5 * dz);
+    const bool xi_enabled = get<bool>(cfg, "xi_guard_enabled", true);
+    if (!xi_guard(dx, dy, dz, rx, ry, rz, a, b, c, T, T_star, modechoice, kappa, L1, L2, L3, xi_enabled)) {
+        std::cout << "\nAborting this run due to correlation-length guard." << std::endl;
+        return 1;
+    }
+    const double W = get<double>(cfg, "W", 0.0);
+    const double gamma = get<double>(cfg, "gamma", 0.1);
+    const int maxIterations = get<int>(cfg, "iterations", 100000);
+    const int printFreq = std::max(1, get<int>(cfg, "print_freq", 200));
+    const double tolerance = get<double>(cfg, "tolerance", 1e-2);
+    const double defect_eps = get<double>(cfg, "defect_density_abs_eps", 1e-4);
+    const bool debug_dynamics = get<bool>(cfg, "debug_dynamics", false);
+    const int sim_mode = get<int>(cfg, "sim_mode", 1);
+    const std::string bmode_raw = get_string(cfg, "boundary_order_mode", "equilibrium");
+    const std::string bmode = lower(trim(bmode_raw));
+    const bool custom = (bmode == "custom" || bmode == "fixed");
+    if (!bmode.empty() && bmode != "equilibrium" && !custom)
+        std::cout << "[Boundary] Unrecognized boundary_order_mode='" << bmode_raw << "'; using equilibrium." << std::endl;
+    double S_custom = 0.0;
+    if (custom) {
+        const double def = equilibrium_shell_order(a, b, c, T, T_star, modechoice);
+        S_custom = get<double>(cfg, "boundary_S", def);
+        if (!std::isfinite(S_custom)) S_custom = def;
+    }
+    auto S_shell_at = [&](double Tv) { return custom ? S_custom : equilibrium_shell_order(a, b, c, Tv, T_star, modechoice); };
+    if (!custom) std::cout << "[Boundary] Shell order policy: equilibrium S_shell = max(S_eq(T), 0)." << std::endl;
+    else std::cout << "[Boundary] Shell order policy: custom S_shell = " << S_custom << std::endl;
+
+    if (dry) {
+        std::cout.precision(17);
+        std::cout << "resolved init_mode=" << mode << "\nresolved random_seed=" << random_seed << "\nresolved grid="
+                  << Nx << "x" << Ny << "x" << Nz << "\nresolved S_eq=" << Seq << "\nresolved S0=" << S0
+                  << "\nresolved kappa=" << kappa << "\nresolved L1=" << L1 << "\nresolved L2=" << L2
+                  << "\nresolved L3=" << L3 << "\nresolved W=" << W << "\nresolved gamma=" << gamma
+                  << "\nresolved sim_mode=" << sim_mode << "\nresolved S_shell=" << S_shell_at(T)
+                  << "\nresolved radius_x=" << rx << std::endl;
+        const DtResult e = estimate_dt(dx, dy, dz, gamma, a, b, c, T_star, modechoice, kappa, L1, L2, L3, S_ref_used,
+                                       S0, T, T, false, 0.0, 0);
+        std::cout << "resolved dt_max=" << e.dt_max << std::endl;
+        return 0;
+    }
+
+    R.Nx = Nx; R.Ny = Ny; R.Nz = Nz;
+    R.n = (long long)Nx * Ny * Nz;
+    R.p = qsr_params{Nx, Ny, Nz, dx, dy, dz, a, b, c, T_star, modechoice, kappa, L1, L2, L3, W, gamma, radius_cells};
+    check(qsr_create(&R.p, &R.h), "qsr_create");
+    qsr_geometry_info geo{};
+    check(qsr_geometry(R.h, &geo), "qsr_geometry");
+    if (W > 0.0) {
+        std::cout << "\n--- Weak Anchoring Shell ---\nShell voxels              = " << geo.shell_cells
+                  << "\nEffective shell thickness = " << geo.delta_eff << " m\nWeak anchoring scale W/δ  = "
+                  << (W / geo.delta_eff) << " J/m^3" << std::endl;
+    }
+
+    std::vector<double> h_Q((size_t)(5 * R.n));
+    auto init_field = [&](double noise_default) {
+        const std::string init_file = get_string(cfg, "init_file", "");
+        if (!init_file.empty()) {
+            std::string err;
+            if (!load_qtensor(init_file, Nx, Ny, Nz, h_Q, err)) throw Fail{"init_file: " + err};
+            std::cout << "[Init] Warm start from " << init_file << std::endl;
+        } else if (mode == 2) {
+            const double amp = get<double>(cfg, "noise_amplitude", noise_default);
+            check(qsr_initial_field(R.h, 2, random_seed, S0, amp, h_Q.data()), "qsr_initial_field");
+        } else {
+            check(qsr_initial_field(R.h, mode, random_seed, S0, 0.0, h_Q.data()), "qsr_initial_field");
+        }
+        check(qsr_upload(R.h, h_Q.data()), "qsr_upload");
+    };
+
+    const int defects_slice_default = Nz / 2;
+
+    if (sim_mode == 3) {
+        // ---------------------------------------------------------------- quench (QSR.cu:2412-2983)
+        const fs::path out_dir = get_string(cfg, "out_dir", "output_quench");
+        if (fs::exists(out_dir) && get<bool>(cfg, "overwrite_out_dir", true)) fs::remove_all(out_dir);
+        fs::create_directories(out_dir);
+        const int protocol = get<int>(cfg, "protocol", 2);
+        const double T_high = get<double>(cfg, "T_high", T);
+        const double T_low = get<double>(cfg, "T_low", T_high - 5.0);
+        const int pre_equil = get<int>(cfg, "pre_equil_iters", 0);
+        int ramp_iters = 0;
+        if (protocol == 2) ramp_iters = std::max(1, get<int>(cfg, "ramp_iters", 1000));
+        const int total_iters = std::max(1, get<int>(cfg, "total_iters", maxIterations));
+        const int logFreq = std::max(1, get<int>(cfg, "logFreq", printFreq));
+        int snapshot_mode = std::min(std::max(get<int>(cfg, "snapshot_mode", 2), 0), 2);
+        int snapshotFreq = 0;
+        if (snapshot_mode == 1) snapshotFreq = std::max(0, get<int>(cfg, "snapshotFreq", 10000));
+        double Tc_KZ = kNaN, Tc_window = 0.0;
+        int kzSnapFreq = 0, kzItersAfterStep = 0, kzExtra = 0;
+        bool kz_stop_early = false, save_q_snaps = false;
+        if (snapshot_mode == 2) {
+            Tc_KZ = get<double>(cfg, "Tc_KZ", 310.2);
+            if (protocol == 2) {
+                Tc_window = std::abs(get<double>(cfg, "Tc_window_K", 0.5));
+                kzSnapFreq = std::max(1, get<int>(cfg, "kzSnapshotFreq", 1000));
+            } else {
+                kzItersAfterStep = std::max(1, get<int>(cfg, "kzItersAfterStep", 200000));
+                kzSnapFreq = std::max(1, get<int>(cfg, "kzSnapshotFreq", 1000));
+            }
+            kz_stop_early = get<bool>(cfg, "kz_stop_early", true);
+            if (kz_stop_early) kzExtra = std::max(0, get<int>(cfg, "kzExtraIters", 0));
+            save_q_snaps = get<bool>(cfg, "save_qtensor_snapshots", false);
+        }
+        init_field(1e-3);
+        const bool semi = get<bool>(cfg, "use_semi_implicit", true);
+        const bool ldg = (L1 != 0.0 || L2 != 0.0 || L3 != 0.0);
+        const double L_base_abs = std::abs(ldg ? L1 : kappa);
+        double L_stab = 0.0;
+        int jacobi = 0;
+        if (semi) {
+            L_stab = get<double>(cfg, "L_stab", L_base_abs > 0.0 ? L_base_abs : 0.0);
+            if (!std::isfinite(L_stab) || L_stab < 0.0) L_stab = 0.0;
+            if (L_base_abs > 0.0 && L_stab > L_base_abs) {
+                std::cout << "[SemiImplicit] Clamping L_stab from " << L_stab << " to |L_base|=" << L_base_abs << std::endl;
+                L_stab = L_base_abs;
+            }
+            jacobi = std::max(0, get<int>(cfg, "jacobi_iters", 25));
+        }
+        const DtResult e = estimate_dt(dx, dy, dz, gamma, a, b, c, T_star, modechoice, kappa, L1, L2, L3, S_ref_used,
+                                       S0, T_high, T_low, semi, L_stab, jacobi);
+        print_dt(e);
+        double dt = get<double>(cfg, "dt", e.dt_max);
+        if (dt > e.dt_max) dt = e.dt_max;
+        const bool guard = get<bool>(cfg, "enable_instability_guard", true);
+        if (cfg.count("enable_adaptive_dt"))
+            std::cout << "[Protocol] Ignoring legacy enable_adaptive_dt=" << cfg.at("enable_adaptive_dt")
+                      << " in quench mode. Kibble-Zurek runs use fixed dt." << std::endl;
+        std::cout << "[Protocol] Quench/KZ runs enforce fixed dt = " << dt << " s." << std::endl;
+        const double S_abort = guard ? get<double>(cfg, "S_abort", 2.0) : 0.0;
+        const double checker_abort = guard ? get<double>(cfg, "checker_rel_abort", 0.10) : 0.0;
+        const bool limiter = get<bool>(cfg, "enable_q_limiter", false);
+        const double S_cap = limiter ? get<double>(cfg, "S_cap", 1.2) : 0.0;
+        const double q_cap = (limiter && S_cap > 0.0) ? S_cap * std::sqrt(2.0 / 3.0) : 0.0;
+        const bool early = get<bool>(cfg, "enable_early_stop", false);
+        const double rad_thr = early ? get<double>(cfg, "radiality_threshold", 0.998) : 0.0;
+        const bool console = get<bool>(cfg, "console_output", true);
+        const bool log_def = get<bool>(cfg, "log_defects_2d", true);
+        const bool track_def = log_def || early;
+        int dz_slice = defects_slice_default;
+        double dthr = 0.1, dcut = 0.25;
+        if (track_def) {
+            dz_slice = std::min(std::max(get<int>(cfg, "defects_z_slice", dz_slice), 0), Nz - 1);
+            dthr = get<double>(cfg, "defects_S_threshold", dthr);
+            dcut = get<double>(cfg, "defects_charge_cutoff", dcut);
+        }
+        const bool log_xi = get<bool>(cfg, "log_xi_grad_2d", true);
+        int xz = dz_slice;
+        double xthr = dthr;
+        if (log_xi) {
+            xz = std::min(std::max(get<int>(cfg, "xi_z_slice", xz), 0), Nz - 1);
+            xthr = get<double>(cfg, "xi_S_threshold", xthr);
+        }
+        // Langevin noise (not in the reference's confined solver): sigma^2 = 2 (1/gamma) noise_strength dt,
+        // the amplitude convention of KZM_bulk_ldg.cu:955-957.
+        const double noise_strength = get<double>(cfg, "noise_strength", 0.0);
+        const double sigma = noise_strength > 0.0 ? std::sqrt(2.0 * (1.0 / gamma) * noise_strength * dt) : 0.0;
+        const unsigned long long noise_seed =
+            (unsigned long long)get<long long>(cfg, "noise_seed", random_seed >= 0 ? random_seed : 0);
+
+        std::ofstream qlog((out_dir / "quench_log.dat").string());
+        qlog << "iteration,time_s,dt_s,T_K,bulk,elastic,anchoring,total,radiality,avg_S,max_S,checker_rel,"
+                "defect_density_per_plaquette,defect_plaquettes_used,xi_grad_proxy,xi_grad_edges_used\n";
+        auto T_at = [&](int it) -> double {
+            if (it < pre_equil) return T_high;
+            if (protocol == 1) return T_low;
+            const int t = it - pre_equil;
+            if (t <= 0) return T_high;
+            if (t >= ramp_iters) return T_low;
+            return T_high + (T_low - T_high) * ((double)t / (double)ramp_iters);
+        };
+        auto reached_final = [&](int it) {
+            if (it < pre_equil) return false;
+            if (protocol == 1) return true;
+            return it >= pre_equil + ramp_iters;
+        };
+        double physical_time = 0.0, prev_F = kNaN, prev_def = kNaN;
+        bool entered = false, aborted = false;
+        int exit_iter = -1;
+        for (int iter = 0; iter < total_iters; ++iter) {
+            const double Tc = T_at(iter);
+            const double S_shell = S_shell_at(Tc);
+            qsr_step_args sa{Tc, S_shell, dt, q_cap, sigma, noise_seed, iter, semi ? 1 : 0, L_stab, jacobi};
+            check(qsr_step(R.h, 1, &sa), "qsr_step");
+            physical_time += dt;
+            const bool do_log = (iter % logFreq == 0) || (iter == total_iters - 1);
+            bool in_win = false, do_snap = false;
+            if (snapshot_mode == 1) {
+                do_snap = (snapshotFreq > 0) && ((iter % snapshotFreq == 0) || (iter == total_iters - 1));
+            } else if (snapshot_mode == 2) {
+                if (protocol == 2) {
+                    if (std::isfinite(Tc_KZ) && std::isfinite(Tc_window) && Tc_window > 0.0) in_win = std::abs(Tc - Tc_KZ) <= Tc_window;
+                    else in_win = std::isfinite(Tc_KZ) ? (std::abs(Tc - Tc_KZ) <= 1e-12) : false;
+                } else {
+                    in_win = (iter >= pre_equil) && (iter <= pre_equil + kzItersAfterStep);
+                }
+                bool in_post = false;
+                if (kz_stop_early && kzExtra > 0 && exit_iter >= 0) in_post = (iter > exit_iter) && (iter <= exit_iter + kzExtra);
+                do_snap = (kzSnapFreq > 0) && ((iter % kzSnapFreq) == 0) && (in_win || in_post);
+            }
+            if (do_log || do_snap) {
+                const qsr_observables o = observe(R, Tc, S_shell, dz_slice, dthr, dcut, xz, xthr, do_log && track_def,
+                                                  do_log && log_xi);
+                const double F = o.total;
+                const double ddens = (do_log && track_def) ? o.defect_density : kNaN;
+                const unsigned long long dplaq = (do_log && track_def) ? (unsigned long long)o.defect_plaquettes : 0ull;
+                const double xiv = (do_log && log_xi) ? o.xi_grad_proxy : kNaN;
+                const unsigned long long xe = (do_log && log_xi) ? (unsigned long long)o.xi_edges : 0ull;
+                const double maxS = o.max_S;
+                const double checker = o.checker_rel;
+                if (do_log) {
+                    qlog << iter << "," << physical_time << "," << dt << "," << Tc << "," << o.bulk << "," << o.elastic
+                         << "," << o.anchoring << "," << F << "," << o.radiality << "," << o.avg_S << "," << maxS << ","
+                         << checker << "," << ddens << "," << dplaq << "," << xiv << "," << xe << "\n";
+                    qlog.flush();
+                    if (console)
+                        std::cout << "Iter " << iter << "  t=" << physical_time << " s  T=" << Tc << " K  F=" << F
+                                  << " (bulk=" << o.bulk << ", el=" << o.elastic << ", anch=" << o.anchoring
+                                  << ")  Rbar=" << o.radiality << "  <S>=" << o.avg_S << "  maxS=" << maxS
+                                  << "  checker=" << checker << std::endl;
+                    if (guard) {
+                        const bool s_bad = !std::isfinite(maxS) || o.nonfinite_cells > 0 || (S_abort > 0.0 && maxS > S_abort);
+                        const bool cb_bad = std::isfinite(checker) && checker_abort > 0.0 && checker > checker_abort;
+                        if (s_bad || cb_bad) {
+                            std::cerr << "\n[InstabilityGuard] Detected runaway/aliasing at iter " << iter
+                                      << ": max_S=" << maxS << ", checker_rel=" << checker << ". dt=" << dt << " s" << std::endl;
+                            aborted = true;
+                            break;
+                        }
+                    }
+                    if (early && reached_final(iter)) {
+                        bool e_conv = false;
+                        if (std::isfinite(prev_F) && prev_F != 0.0) e_conv = std::abs((F - prev_F) / prev_F) < tolerance;
+                        const bool d_conv = dplaq > 0 && std::isfinite(prev_def) && std::isfinite(ddens) &&
+                                            std::abs(ddens - prev_def) < defect_eps;
+                        if (e_conv && d_conv) {
+                            std::cout << "\n=== Early-stop: converged at final T (energy + defect proxy stable; Rbar="
+                                      << o.radiality << ", defect2D=" << ddens << ", radiality_threshold_met="
+                                      << ((rad_thr <= 0.0 || o.radiality > rad_thr) ? "yes" : "no") << ") ===\n";
+                            break;
+                        }
+                        prev_F = F;
+                        prev_def = dplaq > 0 ? ddens : kNaN;
+                    }
+                }
+                if (do_snap) {
+                    save_nematic(nematic(R), Nx, Ny, Nz, (out_dir / ("nematic_field_iter_" + std::to_string(iter) + ".dat")).string());
+                    if (save_q_snaps)
+                        save_qtensor(download(R), Nx, Ny, Nz, (out_dir / ("Qtensor_output_iter_" + std::to_string(iter) + ".dat")).string());
+                }
+            }
+            if (snapshot_mode == 2 && kz_stop_early) {
+                if (protocol == 2) {
+                    if (in_win) entered = true;
+                    const bool below = (std::isfinite(Tc_KZ) && std::isfinite(Tc_window)) ? (Tc < Tc_KZ - Tc_window) : false;
+                    if (entered && !in_win && below) {
+                        if (exit_iter < 0) exit_iter = iter;
+                        if (iter >= exit_iter + kzExtra) {
+                            std::cout << "\n=== KZ mode: stopping after leaving Tc window ===\n";
+                            break;
+                        }
+                    }
+                } else if (iter >= pre_equil + kzItersAfterStep + kzExtra) {
+                    std::cout << "\n=== KZ mode: stopping after post-step recording window ===\n";
+                    break;
+                }
+            }
+        }
+        if (aborted) {
+            qlog.close();
+            std::cerr << "[Quench] Run aborted by the fixed-dt instability guard. Final state was not saved." << std::endl;
+            return 1;
+        }
+        save_nematic(nematic(R), Nx, Ny, Nz, (out_dir / "nematic_field_final.dat").string());
+        save_qtensor(download(R), Nx, Ny, Nz, (out_dir / "Qtensor_output_final.dat").string());
+        qlog.close();
+    } else if (sim_mode == 2) {
+        // ------------------------------------------------------------ sweep (QSR.cu:2985-3124)
+        if (fs::exists("output_temp_sweep")) fs::remove_all("output_temp_sweep");
+        fs::create_directory("output_temp_sweep");
+        std::ofstream sweep_log("output_temp_sweep/summary.dat");
+        sweep_log << "temperature,final_energy_including_anchoring,average_S\n";
+        const double T_start = get<double>(cfg, "T_start", 295.0), T_end = get<double>(cfg, "T_end", 315.0);
+        double T_step = get<double>(cfg, "T_step", 1.0);
+        if (T_step == 0.0) {
+            std::cout << "Step T cannot be 0. Aborting sweep." << std::endl;
+            return 0;
+        }
+        if ((T_end - T_start) * T_step < 0.0) T_step = -T_step;
+        init_field(1e-3);
+        const DtResult e = estimate_dt(dx, dy, dz, gamma, a, b, c, T_star, modechoice, kappa, L1, L2, L3, S_ref_used,
+                                       S0, T_start, T_end, false, 0.0, 0);
+        print_dt(e);
+        double dt = get<double>(cfg, "dt", e.dt_max);
+        if (dt > e.dt_max) dt = e.dt_max;
+        const double tau_align = (std::min({rx, ry, rz}) * std::min({rx, ry, rz})) / e.D_total;
+        const double min_time = 0.25 * tau_align;
+        auto done = [&](double Tv) { return (T_step > 0.0) ? (Tv > T_end + 1e-12) : (Tv < T_end - 1e-12); };
+        for (double Tc = T_start; !done(Tc); Tc += T_step) {
+            const double S_shell = S_shell_at(Tc);
+            std::cout << "\n--- Running simulation for T = " << Tc << " K with S_shell = " << S_shell << " ---\n";
+            const std::string temp_dir = "output_temp_sweep/T_" + std::to_string(Tc);
+            fs::create_directory(temp_dir);
+            double prev_F = std::numeric_limits<double>::max(), ptime = 0.0;
+            for (int iter = 0; iter < maxIterations; ++iter) {
+                qsr_step_args sa{Tc, S_shell, dt, 0.0, 0.0, 0ull, iter, 0, 0.0, 0};
+                check(qsr_step(R.h, 1, &sa), "qsr_step");
+                ptime += dt;
+                if (iter > 0 && iter % printFreq == 0) {
+                    const double F = observe(R, Tc, S_shell, defects_slice_default, 0.1, 0.25, defects_slice_default,
+                                             0.1, false, false).total;
+                    std::cout << "  Iter " << iter << ", Free Energy: " << F << std::endl;
+                    if (ptime >= min_time && prev_F != 0.0 && (std::abs((F - prev_F) / prev_F) < tolerance || F == 0.0)) {
+                        std::cout << "  Convergence reached at iteration " << iter << std::endl;
+                        break;
+                    }
+                    prev_F = F;
+                }
+            }
+            const qsr_observables o = observe(R, Tc, S_shell, defects_slice_default, 0.1, 0.25, defects_slice_default,
+                                              0.1, false, false);
+            sweep_log << Tc << "," << o.total << "," << o.avg_S << "\n";
+            sweep_log.flush();
+            save_nematic(nematic(R), Nx, Ny, Nz, temp_dir + "/nematic_field_final.dat");
+            save_qtensor(download(R), Nx, Ny, Nz, temp_dir + "/Qtensor_output_final.dat");
+            std::cout << "  Saved final state for T = " << Tc << " K. Average S = " << o.avg_S << std::endl;
+        }
+    } else {
+        // ------------------------------------------------------- single T (QSR.cu:3126-3476)
+        int submode = get<int>(cfg, "submode", 1);
+        if (submode != 1 && submode != 2) submode = 1;
+        std::cout << "Submode selected: " << (submode == 1 ? "full energy" : "energy components") << std::endl;
+        if (fs::exists("output"))
+            for (const auto& entry : fs::directory_iterator("output")) fs::remove(entry.path());
+        fs::create_directory("output");
+        const DtResult e = estimate_dt(dx, dy, dz, gamma, a, b, c, T_star, modechoice, kappa, L1, L2, L3, S_ref_used,
+                                       S0, T, T, false, 0.0, 0);
+        const double R_phys = std::min({rx, ry, rz});
+        const double tau_align = (R_phys * R_phys) / e.D_total;
+        std::cout << "\n--- Time Scale Analysis ---\nDiffusion coefficient D = " << e.D_total
+                  << " m²/s\nDroplet radius R ≈ " << R_phys << " m\nEstimated alignment time τ_align ≈ " << tau_align
+                  << " s" << std::endl;
+        print_dt(e);
+        double dt = get<double>(cfg, "dt", e.dt_max);
+        if (dt > e.dt_max) dt = e.dt_max;
+        init_field(1e-3);
+        const double S_shell = S_shell_at(T);
+        std::cout << "[Boundary] Single-temp shell order at T=" << T << " K: S_shell=" << S_shell << std::endl;
+        const bool console = get<bool>(cfg, "console_output", true);
+        const int dz_slice = std::min(std::max(get<int>(cfg, "defects_z_slice", defects_slice_default), 0), Nz - 1);
+        const double dthr = get<double>(cfg, "defects_S_threshold", 0.1);
+        const double dcut = get<double>(cfg, "defects_charge_cutoff", 0.25);
+        const bool log_xi = get<bool>(cfg, "log_xi_grad_2d", true);
+        int xz = dz_slice;
+        double xthr = dthr;
+        if (log_xi) {
+            xz = std::min(std::max(get<int>(cfg, "xi_z_slice", xz), 0), Nz - 1);
+            xthr = get<double>(cfg, "xi_S_threshold", xthr);
+        }
+        const bool iter_snaps = get<bool>(cfg, "write_iteration_snapshots", true);
+        const std::string log_name = submode == 1 ? "free_energy_vs_iteration.dat" : "energy_components_vs_iteration.dat";
+        std::ofstream elog(log_name);
+        elog << "iteration,bulk,elastic,anchoring,total,radiality,time,avg_S,max_S,defect_density_per_plaquette,"
+                "defect_plaquettes_used,xi_grad_proxy,xi_grad_edges_used\n";
+        double prev_F = std::numeric_limits<double>::max(), prev_def = kNaN, ptime = 0.0;
+        const double min_time = 0.5 * tau_align;
+        std::vector<double> prev_Q;
+        for (int iter = 0; iter < maxIterations; ++iter) {
+            ptime += dt;
+            qsr_step_args sa{T, S_shell, dt, 0.0, 0.0, 0ull, iter, 0, 0.0, 0};
+            check(qsr_step(R.h, 1, &sa), "qsr_step");
+            if (iter % printFreq == 0) {
+                const qsr_observables o = observe(R, T, S_shell, dz_slice, dthr, dcut, xz, xthr, true, log_xi);
+                const double xiv = log_xi ? o.xi_grad_proxy : kNaN;
+                const unsigned long long xe = log_xi ? (unsigned long long)o.xi_edges : 0ull;
+                if (debug_dynamics) {
+                    std::vector<double> q = download(R);
+                    double max_dQ = 0.0;
+                    if (!prev_Q.empty())
+                        for (size_t t = 0; t < q.size() / 5; ++t) {
+                            double d[5];
+                            for (int m = 0; m < 5; ++m) d[m] = q[5 * t + m] - prev_Q[5 * t + m];
+                            const double zz = -d[0] - d[3];
+                            max_dQ = std::max(max_dQ, std::sqrt(d[0] * d[0] + d[3] * d[3] + zz * zz +
+                                                                2.0 * (d[1] * d[1] + d[2] * d[2] + d[4] * d[4])));
+                        }
+                    prev_Q.swap(q);
+                    std::cout << "  [debug] max|mu|=n/a (fused step)  max|Q|=" << o.max_q_norm << "  max|ΔQ|=" << max_dQ
+                              << std::endl;
+                }
+                elog << iter << "," << o.bulk << "," << o.elastic << "," << o.anchoring << "," << o.total << ","
+                     << o.radiality << "," << ptime << "," << o.avg_S << "," << o.max_S << "," << o.defect_density
+                     << "," << o.defect_plaquettes << "," << xiv << "," << xe << "\n";
+                if (console)
+                    std::cout << "Iter " << iter << "  t=" << ptime << " s  F=" << o.total << " (bulk=" << o.bulk
+                              << ", el=" << o.elastic << ", anch=" << o.anchoring << ")  R̄=" << o.radiality
+                              << "  <S>=" << o.avg_S << "  maxS=" << o.max_S << "  defect2D=" << o.defect_density
+                              << "  xiGrad=" << xiv << std::endl;
+                if (iter_snaps)
+                    save_nematic(nematic(R), Nx, Ny, Nz, "output/nematic_field_iter_" + std::to_string(iter) + ".dat");
+                if (iter > 100 && prev_F != 0.0) {
+                    const bool e_conv = std::abs((o.total - prev_F) / prev_F) < tolerance;
+                    const bool t_ok = ptime > min_time;
+                    const bool d_conv = o.defect_plaquettes > 0 && std::isfinite(prev_def) &&
+                                        std::isfinite(o.defect_density) && std::abs(o.defect_density - prev_def) < defect_eps;
+                    if (e_conv && d_conv && t_ok) {
+                        std::cout << "\n=== Convergence Achieved (energy + defect proxy stable; Rbar=" << o.radiality
+                                  << ", defect2D=" << o.defect_density << ", radiality_threshold_met="
+                                  << (o.radiality > 0.998 ? "yes" : "no") << ") ===";
+                        break;
+                    }
+                }
+                prev_F = o.total;
+                prev_def = o.defect_plaquettes > 0 ? o.defect_density : kNaN;
+            }
+        }
+        elog.close();
+        save_nematic(nematic(R), Nx, Ny, Nz, "nematic_field_final.dat");
+        save_qtensor(download(R), Nx, Ny, Nz, "Qtensor_output_final.dat");
+    }
+    std::cout << "\nSimulation finished." << std::endl;
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    try {
+        return run_main(argc, argv);
+    } catch (const Fail& f) {
+        std::cerr << "[qsr_b200] " << f.msg << std::endl;
+        return 1;
+    }
+}

@@ -55,10 +55,11 @@ def main(outdir=HERE):
                 ref.step(c["T"], S_shell, dt)
         q1 = ref.download()
         obs = ref.observe(c["T"], S_shell, Nz // 2)
+        delta_eff = ref.L.qref_delta_eff()
         ref.destroy()
         np.savez_compressed(os.path.join(outdir, f"qsr_{name}.npz"), q_final=q1, init_sha=_sha(q0),
                             grid=np.array(c["grid"]), T=c["T"], S_shell=S_shell, dt=dt, steps=c["steps"],
-                            imex=int(c["imex"]), params=repr(c["p"]), delta_eff=ref.L.qref_delta_eff(),
+                            imex=int(c["imex"]), params=repr(c["p"]), delta_eff=delta_eff,
                             **{f"obs_{k}": v for k, v in obs.items()})
         print("wrote", name, obs["bulk"], obs["elastic"], obs["anchoring"])
     kref = RefKZM()

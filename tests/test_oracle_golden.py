@@ -29,7 +29,8 @@ def test_oracle_matches_reference_cuda_fixture(oracle, path):
     p = ast.literal_eval(str(z["params"]))
     op = make_params(Nx=Nx, Ny=Ny, Nz=Nz, T_star=307.0, **p)
     g, fl = oracle.geometry(op)
-    assert g.delta_eff == pytest.approx(float(z["delta_eff"]), rel=1e-14)
+    if float(z["delta_eff"]) != 0.0:  # recorded by the generator
+        assert g.delta_eff == pytest.approx(float(z["delta_eff"]), rel=1e-14)
     q0 = oracle.init(op, g, 0, 42, 0.5)
     assert _sha(q0) == str(z["init_sha"]), "initial field differs from the one the fixture was made from"
     T, S, dt, steps = float(z["T"]), float(z["S_shell"]), float(z["dt"]), int(z["steps"])
