@@ -163,6 +163,19 @@ int kzm_download(kzm_handle* h, double* q_aos5);
 int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* args);
 /* Replaces the full D2H + host compute_observables (KZM_bulk_ldg.cu:923-925, 543-713). */
 int kzm_observe(kzm_handle* h, double A, double B, double C, kzm_observables* out);
+/* No counterpart in the reference. The observables of kzm_observe computed straight from a
+ * field the caller keeps in device memory (the reference's own layout: AoS FP64, 5 doubles per
+ * site, x fastest), for callers that must not allocate device memory: code running under
+ * another framework's memory pool, or a loop that is being captured into a CUDA graph. It
+ * calls no cudaMalloc/cudaFree: its scratch is a fixed file-scope device array in this
+ * library, sized for at most KZM_NOALLOC_MAX_SITES sites (larger grids get LDG_ERR_ARG).
+ * The first call on each device looks up that array's device address, so make that first
+ * call before any stream capture. All calls share the array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialised by the caller. Work runs
+ * on `stream` (a cudaStream_t, NULL = legacy default stream); the call synchronises it. */
+#define KZM_NOALLOC_MAX_SITES (1LL << 19)
+int kzm_observe_device_noalloc(const kzm_params* params, const double* q_aos5_device, double A, double B,
+                               double C, void* stream, kzm_observables* out);
 void* kzm_stream(kzm_handle* h);
 long long kzm_launch_count(const kzm_handle* h);
 int kzm_destroy(kzm_handle* h);

@@ -7,7 +7,9 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <new>
+#include <string>
 
 #include "ldg_api_common.h"
 #include "ldg_common.cuh"
@@ -175,6 +177,67 @@ __global__ void __launch_bounds__(kThreads) k_kzm_obs_sites(const float* __restr
             d[m][0] = ((double)b[px] - c[m]) * O.ix;
             d[m][1] = ((double)b[py] - c[m]) * O.iy;
             d[m][2] = ((double)b[pz] - c[m]) * O.iz;
+        }
+#pragma unroll
+        for (int w = 0; w < 3; ++w) d[5][w] = -(d[0][w] + d[3][w]);
+        const double Qxx = c[0], Qxy = c[1], Qxz = c[2], Qyy = c[3], Qyz = c[4], Qzz = -Qxx - Qyy;
+        const double q2xx = Qxx * Qxx + Qxy * Qxy + Qxz * Qxz;
+        const double q2xy = Qxx * Qxy + Qxy * Qyy + Qxz * Qyz;
+        const double q2xz = Qxx * Qxz + Qxy * Qyz + Qxz * Qzz;
+        const double q2yy = Qxy * Qxy + Qyy * Qyy + Qyz * Qyz;
+        const double q2yz = Qxy * Qxz + Qyy * Qyz + Qyz * Qzz;
+        const double q2zz = Qxz * Qxz + Qyz * Qyz + Qzz * Qzz;
+        const double trQ2 = Qxx * Qxx + Qyy * Qyy + Qzz * Qzz + 2.0 * (Qxy * Qxy + Qxz * Qxz + Qyz * Qyz);
+        const double trQ3 = Qxx * q2xx + Qxy * q2xy + Qxz * q2xz + Qxy * q2xy + Qyy * q2yy + Qyz * q2yz +
+                            Qxz * q2xz + Qyz * q2yz + Qzz * q2zz;
+        a.bulk += ((O.A / 2.0) * trQ2 - (O.B / 3.0) * trQ3 + (O.C / 4.0) * trQ2 * trQ2) * O.cv;
+        double g2 = 0.0;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            const double s = d[m][0] * d[m][0] + d[m][1] * d[m][1] + d[m][2] * d[m][2];
+            g2 += (m == 1 || m == 2 || m == 4) ? 2.0 * s : s;
+        }
+        a.gint += g2 * O.cv;
+        a.elastic += 0.5 * O.kappa * g2 * O.cv;
+        a.qint += trQ2 * O.cv;
+        const Nematic f = nematic64(c, 1e-12, Nematic{0.0, 1.0, 0.0, 0.0});
+        nf[t] = make_double4(f.S, f.nx, f.ny, f.nz);
+        a.S_sum += f.S;
+        a.S_max = fmax(a.S_max, f.S);
+    }
+    __shared__ double shd[kThreads / 32];
+    KzmPartial res{};
+    res.bulk = bsum(a.bulk, shd);
+    res.elastic = bsum(a.elastic, shd);
+    res.qint = bsum(a.qint, shd);
+    res.gint = bsum(a.gint, shd);
+    res.S_sum = bsum(a.S_sum, shd);
+    res.S_max = bmax(a.S_max, shd);
+    if (threadIdx.x == 0) part[blockIdx.x] = res;
+}
+
+// Pass 1 on a caller-owned device field in the reference layout (AoS FP64, x fastest).
+__global__ void __launch_bounds__(kThreads) k_kzm_obs_sites_aos(const double* __restrict__ q, KzmObsConst O,
+                                                                double4* __restrict__ nf,
+                                                                KzmPartial* __restrict__ part) {
+    const KzmConst& P = O.P;
+    const long long n = (long long)P.Nx * P.Ny * P.Nz;
+    KzmPartial a{};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(t % P.Nx);
+        const long long r = t / P.Nx;
+        const int y = (int)(r % P.Ny);
+        const int z = (int)(r / P.Ny);
+        const long long px = (long long)((x + 1) % P.Nx) + (long long)P.Nx * ((long long)y + (long long)P.Ny * z);
+        const long long py = (long long)x + (long long)P.Nx * ((long long)((y + 1) % P.Ny) + (long long)P.Ny * z);
+        const long long pz = (long long)x + (long long)P.Nx * ((long long)y + (long long)P.Ny * ((z + 1) % P.Nz));
+        double c[5], d[6][3];
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            c[m] = q[5 * t + m];
+            d[m][0] = (q[5 * px + m] - c[m]) * O.ix;
+            d[m][1] = (q[5 * py + m] - c[m]) * O.iy;
+            d[m][2] = (q[5 * pz + m] - c[m]) * O.iz;
         }
 #pragma unroll
         for (int w = 0; w < 3; ++w) d[5][w] = -(d[0][w] + d[3][w]);
@@ -463,6 +526,91 @@ int kzm_observe(kzm_handle* h, double A, double B, double C, kzm_observables* o)
     o->elastic = R.elastic / tv;
     o->total = o->bulk + o->elastic;
     o->avg_S = R.S_sum / (double)h->n;
+    o->max_S = R.S_max;
+    o->defect_plaquettes_used = (long long)R.used;
+    o->nonzero_defect_plaquettes = (long long)R.defects;
+    o->defect_density_per_plaquette = R.used > 0 ? (double)R.defects / (double)R.used : nan;
+    o->defect_line_density = tv > 0.0 ? R.line / tv : nan;
+    o->xi_grad_proxy = (R.gint > 0.0 && R.qint > 0.0) ? std::sqrt(R.qint / R.gint) : nan;
+    return LDG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// No-allocation observables. Scratch lives in file-scope device arrays of this library:
+// the per-site nematic field of at most KZM_NOALLOC_MAX_SITES sites (16 MiB) and one
+// partial per reduction block. Every slot a kernel reads is written earlier in the same
+// call (all sites of the grid, all kBlocks partials and the final slot), so nothing has to
+// start at zero; the arrays keep the last call's contents.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) double4 g_noalloc_nematic[KZM_NOALLOC_MAX_SITES];
+static __device__ __align__(256) KzmPartial g_noalloc_partials[kBlocks + 1];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double4* g_noalloc_nematic_ptr[kMaxDevices] = {};
+KzmPartial* g_noalloc_partials_ptr[kMaxDevices] = {};
+
+// Device addresses of the scratch arrays for the current device, looked up once per device.
+int noalloc_scratch(double4** nf, KzmPartial** part) {
+    int dev = 0;
+    LDG_CUDA(cudaGetDevice(&dev));
+    LDG_REQUIRE(dev >= 0 && dev < kMaxDevices, LDG_ERR_ARG, "kzm_observe_device_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_nematic_ptr[dev]) {
+        void* a = nullptr;
+        void* b = nullptr;
+        LDG_CUDA(cudaGetSymbolAddress(&a, g_noalloc_nematic));
+        LDG_CUDA(cudaGetSymbolAddress(&b, g_noalloc_partials));
+        g_noalloc_nematic_ptr[dev] = static_cast<double4*>(a);
+        g_noalloc_partials_ptr[dev] = static_cast<KzmPartial*>(b);
+    }
+    *nf = g_noalloc_nematic_ptr[dev];
+    *part = g_noalloc_partials_ptr[dev];
+    return LDG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int kzm_observe_device_noalloc(const kzm_params* params, const double* q, double A, double B, double C,
+                               void* stream, kzm_observables* o) {
+    clear_error();
+    LDG_REQUIRE(params && q && o, LDG_ERR_ARG, "kzm_observe_device_noalloc: null argument");
+    const kzm_params& p = *params;
+    LDG_REQUIRE(p.Nx > 1 && p.Ny > 1 && p.Nz > 1, LDG_ERR_ARG,
+                "Nx, Ny, and Nz must all be greater than 1 for the periodic bulk LdG branch");
+    LDG_REQUIRE(p.dx > 0 && p.dy > 0 && p.dz > 0, LDG_ERR_ARG, "dx, dy, and dz must be positive");
+    const long long n = (long long)p.Nx * p.Ny * p.Nz;
+    LDG_REQUIRE(n <= KZM_NOALLOC_MAX_SITES, LDG_ERR_ARG,
+                "kzm_observe_device_noalloc: " + std::to_string(n) + " sites exceed the no-allocation scratch limit of " +
+                    std::to_string(KZM_NOALLOC_MAX_SITES) + " sites (use kzm_observe for larger grids)");
+    double4* nf = nullptr;
+    KzmPartial* part = nullptr;
+    int rc = noalloc_scratch(&nf, &part);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    KzmObsConst O{};
+    O.P.Nx = p.Nx; O.P.Ny = p.Ny; O.P.Nz = p.Nz;
+    O.A = A; O.B = B; O.C = C; O.kappa = p.kappa;
+    O.cv = p.dx * p.dy * p.dz;
+    O.ix = 1.0 / p.dx; O.iy = 1.0 / p.dy; O.iz = 1.0 / p.dz;
+    k_kzm_obs_sites_aos<<<kBlocks, kThreads, 0, st>>>(q, O, nf, part);
+    k_kzm_obs_plaq<<<kBlocks, kThreads, 0, st>>>(nf, O, p.defects_S_threshold, p.defects_charge_cutoff, p.dx, p.dy,
+                                                  p.dz, part);
+    k_kzm_obs_final<<<1, kThreads, 0, st>>>(part, kBlocks, part + kBlocks);
+    LDG_LAUNCHED("kzm_observe_device_noalloc kernels");
+    KzmPartial R{};
+    LDG_CUDA(cudaMemcpyAsync(&R, part + kBlocks, sizeof(R), cudaMemcpyDeviceToHost, st));
+    LDG_CUDA(cudaStreamSynchronize(st));
+    const double tv = O.cv * (double)p.Nx * (double)p.Ny * (double)p.Nz;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    o->bulk = R.bulk / tv;
+    o->elastic = R.elastic / tv;
+    o->total = o->bulk + o->elastic;
+    o->avg_S = R.S_sum / (double)n;
     o->max_S = R.S_max;
     o->defect_plaquettes_used = (long long)R.used;
     o->nonzero_defect_plaquettes = (long long)R.defects;
