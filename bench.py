@@ -48,7 +48,105 @@ WORKLOADS = {
                     droplet_radius_cells=28.0),
         T=300.0, S_shell=None, S0=0.5, seed=42),
 }
+WORKLOADS["periodic_quench_512"] = dict(
+    kind="periodic",
+    desc="512^3 periodic bulk LdG, kappa=6e-12 N, gamma=0.1, linear ramp 315->295 K over 1e4 steps, "
+         "Langevin noise_strength=kT/dx^3 (300 K), init N(0,1e-3) seed 12345",
+    N=512, d=1e-8, kappa=6e-12, gamma=0.1, a=0.044e6, b=1.413e6, c=1.153e6, T_star=307.0, T_high=315.0,
+    T_low=295.0, ramp=10000, amp=1e-3, seed=12345, log_every=100)
 DEFAULT_WORKLOAD = "anisotropic_weak_256"
+
+
+def bench_periodic(args, w, torch, pg, rank, world, local):
+    """Periodic bulk quench (the KZM_bulk_ldg path): one kzm_step kernel per step."""
+    import lcdrsimulator_b200 as L
+    from lcdrsimulator_b200.physics import bulk_ABC, S_eq
+    N, d = w["N"], w["d"]
+    # rough explicit limit of the reference (KZM_bulk_ldg.cu:330-349)
+    Ah = bulk_ABC(w["a"], w["b"], w["c"], w["T_high"], w["T_star"])[0]
+    Al, Bl, Cl = bulk_ABC(w["a"], w["b"], w["c"], w["T_low"], w["T_star"])
+    Sl = S_eq(Al, Bl, Cl)
+    stiff = (1.0 / w["gamma"]) * (2.0 * w["kappa"] * 3.0 / (d * d) + max(abs(Ah), abs(Al)) + abs(Bl) * abs(Sl) +
+                                  abs(Cl) * 2.0 * Sl * Sl / 3.0)
+    dt = 0.2 / stiff
+    kT = 1.380649e-23 * 300.0
+    sigma = math.sqrt(2.0 * (1.0 / w["gamma"]) * (kT / d ** 3) * dt)
+    s = L.KZMSolver(N, N, N, d, d, d, w["kappa"], w["gamma"])
+    rng = np.random.default_rng(w["seed"])
+    q0 = w["amp"] * rng.standard_normal(5 * N ** 3)
+    s.upload(q0)
+    stream = torch.cuda.ExternalStream(s.stream())
+
+    def T_at(it):
+        if it >= w["ramp"]:
+            return w["T_low"]
+        return w["T_high"] + (w["T_low"] - w["T_high"]) * it / w["ramp"]
+
+    def step(it):
+        A, B, C = bulk_ABC(w["a"], w["b"], w["c"], T_at(it), w["T_star"])
+        s.step(1, A, B, C, dt, noise_sigma=sigma, seed=w["seed"], step_index=it)
+
+    for it in range(args.warmup):
+        step(it)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = s.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for it in range(args.warmup, args.warmup + args.steps):
+        step(it)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    launches = s.launch_count() - l0
+    sites = N ** 3
+    t_step = ms / 1e3 / args.steps
+    peak, peak_kind = load_peaks()
+    alg = BYTES_PER_CELL * sites
+    e2e = None
+    if not args.no_e2e:
+        q_in = torch.from_numpy(q0).pin_memory().numpy()
+        q_out = torch.empty(q0.size, dtype=torch.float64).pin_memory().numpy()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.upload(q_in)
+        n_obs = 0
+        for it in range(args.steps):
+            step(it)
+            if it % w["log_every"] == 0:
+                A, B, C = bulk_ABC(w["a"], w["b"], w["c"], T_at(it), w["T_star"])
+                s.observe(A, B, C)
+                n_obs += 1
+        s.download(q_out)
+        e1.record(stream)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1)
+        e2e = {"value": world * sites * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": (40 * sites + args.steps * 56) / args.steps,
+               "d2h_bytes_per_step": (40 * sites + n_obs * 80) / args.steps,
+               "note": "kzm_upload + K x kzm_step + kzm_observe every 100 steps + kzm_download"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": world * sites * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": args.workload, "desc": w["desc"], "grid": [N, N, N], "dt_s": dt,
+                           "noise_sigma": sigma, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (two 5-component FP32 fields of 2.7 GB)"},
+                "roofline": {"bound": "hbm", "achieved": alg / t_step / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": alg / t_step / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                             "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
+                "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    s.close()
+    return 0
 
 
 def dt_max(w):
@@ -215,6 +313,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
         pg = dist
     import lcdrsimulator_b200 as L
+
+    if w.get("kind") == "periodic":
+        return bench_periodic(args, w, torch, pg, rank, world, local)
 
     solver = L.QSRSolver(**w["params"])
     geo = solver.geometry()

@@ -89,6 +89,110 @@ __global__ void __launch_bounds__(256) k_kzm_step(const float* __restrict__ q, f
     for (int m = 0; m < 5; ++m) out[m * P.sc + id] = u[m];
 }
 
+// The same step as k_kzm_step for a (32 x 8) column tile marching along z over a chunk of
+// planes. Each thread keeps its column's planes z-1, z, z+1 in registers and prefetches
+// z+2 and z+3; the x/y neighbours come from a shared (34 x 10) tile whose halo holds the
+// periodically wrapped values (any N >= 2). Every input value is loaded about once from
+// HBM (halo columns from L2) and every site is written once.
+constexpr int KTX = 32, KTY = 8, KZC = 32;
+template <bool kNoise>
+__global__ void __launch_bounds__(KTX* KTY) k_kzm_step_tiled(const float* __restrict__ q, float* __restrict__ out,
+                                                             KzmConst P) {
+    __shared__ float s[5][KTY + 2][KTX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * KTX, y0 = blockIdx.y * KTY, z0 = blockIdx.z * KZC;
+    const int z1 = min(z0 + KZC, P.Nz);
+    const int xr = x0 + tx, yr = y0 + ty;
+    const bool valid = (xr < P.Nx) && (yr < P.Ny);
+    const int x = xr % P.Nx, y = yr % P.Ny;
+    const long long row = (long long)y * P.sy;
+    const long long rowm = (long long)((y0 + P.Ny - 1) % P.Ny) * P.sy;   // halo row y0-1
+    const long long rowp = (long long)((y0 + KTY) % P.Ny) * P.sy;        // halo row y0+KTY
+    const int xm = (x0 + P.Nx - 1) % P.Nx, xp = (x0 + KTX) % P.Nx;       // halo columns
+    auto zw = [&](int z) { return (z % P.Nz + P.Nz) % P.Nz; };
+    auto load5 = [&](int z, float v[5]) {
+        const long long o = (long long)zw(z) * P.sz + row + x;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) v[m] = __ldg(q + m * P.sc + o);
+    };
+    float qm[5], qc[5], qp[5], qn[5], qn2[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    load5(z0 - 1, qm);
+    load5(z0, qc);
+    load5(z0 + 1, qp);
+    load5(z0 + 2, qn);
+    const uint32_t cell_base = (uint32_t)(x + P.Nx * y);
+    for (int z = z0; z < z1; ++z) {
+        if (z + 3 < z1 + 1) load5(z + 3, qn2);
+        const long long pz = (long long)zw(z) * P.sz;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) s[m][ty + 1][tx + 1] = qc[m];
+        if (ty == 0) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s[m][0][tx + 1] = __ldg(q + m * P.sc + pz + rowm + x);
+        }
+        if (ty == KTY - 1) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s[m][KTY + 1][tx + 1] = __ldg(q + m * P.sc + pz + rowp + x);
+        }
+        if (tx == 0) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s[m][ty + 1][0] = __ldg(q + m * P.sc + pz + row + xm);
+        }
+        if (tx == KTX - 1) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) s[m][ty + 1][KTX + 1] = __ldg(q + m * P.sc + pz + row + xp);
+        }
+        __syncthreads();
+        if (valid) {
+            float lap[5];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                const float c = qc[m];
+                lap[m] = (s[m][ty + 1][tx + 2] - 2.0f * c + s[m][ty + 1][tx]) * P.ix2 +
+                         (s[m][ty + 2][tx + 1] - 2.0f * c + s[m][ty][tx + 1]) * P.iy2 +
+                         (qp[m] - 2.0f * c + qm[m]) * P.iz2;
+            }
+            float h[6];
+            bulk_field(qc, P.A, P.B, P.C, h);
+            h[0] -= P.kappa * lap[0];
+            h[1] -= P.kappa * lap[3];
+            h[2] += P.kappa * (lap[0] + lap[3]);
+            h[3] -= P.kappa * lap[1];
+            h[4] -= P.kappa * lap[2];
+            h[5] -= P.kappa * lap[4];
+            const float corr = (h[0] + h[1] + h[2]) / 3.0f;
+            float u[5] = {qc[0] - P.mob_dt * (h[0] - corr), qc[1] - P.mob_dt * h[3], qc[2] - P.mob_dt * h[4],
+                          qc[3] - P.mob_dt * (h[1] - corr), qc[4] - P.mob_dt * h[5]};
+            if (kNoise) {
+                float g[5];
+                normals5(cell_base + (uint32_t)P.Nx * (uint32_t)P.Ny * (uint32_t)z, 0u, P.step, P.key0, P.key1, g);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) u[m] += P.sigma * g[m];
+            }
+            if (P.qcap > 0.0f) {
+                const float zz = -u[0] - u[3];
+                const float tr = u[0] * u[0] + u[3] * u[3] + zz * zz + 2.0f * (u[1] * u[1] + u[2] * u[2] + u[4] * u[4]);
+                const float qn_ = sqrtf(fmaxf(tr, 0.0f));
+                if (qn_ > P.qcap && qn_ > 0.0f) {
+                    const float sc = P.qcap / qn_;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) u[m] *= sc;
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) out[m * P.sc + pz + row + x] = u[m];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 5; ++m) {
+            qm[m] = qc[m];
+            qc[m] = qp[m];
+            qp[m] = qn[m];
+            qn[m] = qn2[m];
+        }
+    }
+}
+
 __global__ void k_kzm_from_aos(const double* __restrict__ aos, float* __restrict__ a, KzmConst P) {
     const long long n = (long long)P.Nx * P.Ny * P.Nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -486,10 +590,18 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
     P.sigma = (float)a->noise_sigma;
     P.key0 = (uint32_t)a->seed;
     P.key1 = (uint32_t)(a->seed >> 32);
+    // Tiled z-marching kernel by default; LDG_KZM_KERNEL=direct selects the one-thread-per-site kernel.
+    const char* ksel = getenv("LDG_KZM_KERNEL");
+    const bool direct = ksel && std::strcmp(ksel, "direct") == 0;
     dim3 blk(32, 8, 1), grd((P.Nx + 31) / 32, (P.Ny + 7) / 8, P.Nz);
+    dim3 tgrd((P.Nx + KTX - 1) / KTX, (P.Ny + KTY - 1) / KTY, (P.Nz + KZC - 1) / KZC);
     for (int s = 0; s < n_steps; ++s) {
         P.step = a->step_index + s;
-        if (a->noise_sigma > 0.0) k_kzm_step<true><<<grd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
+        const bool noise = a->noise_sigma > 0.0;
+        if (!direct) {
+            if (noise) k_kzm_step_tiled<true><<<tgrd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
+            else k_kzm_step_tiled<false><<<tgrd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
+        } else if (noise) k_kzm_step<true><<<grd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
         else k_kzm_step<false><<<grd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
         h->launches++;
         LDG_LAUNCHED("k_kzm_step");

@@ -96,37 +96,42 @@ __device__ __forceinline__ void normals5(uint32_t cell, uint32_t instance, long 
 
 // Second derivative along one axis with the reference's shifted stencil at the faces
 // (QSR.cu:296-320).
-template <int AX, class Acc>
+// kFaces = false is the interior form: the caller guarantees 0 < pos < n - 1 for every
+// position the stencil is evaluated at, so the face branches are compiled out.
+template <int AX, bool kFaces = true, class Acc>
 __device__ __forceinline__ float d2_face(const Acc& A, int c, float cv, int pos, int n, float inv) {
     auto at = [&](int s) { return AX == 0 ? A(c, s, 0, 0) : (AX == 1 ? A(c, 0, s, 0) : A(c, 0, 0, s)); };
-    if (pos > 0 && pos < n - 1) return (at(1) - cv * 2.0f + at(-1)) * inv;
+    if (!kFaces || (pos > 0 && pos < n - 1)) return (at(1) - cv * 2.0f + at(-1)) * inv;
     if (pos == 0) return (at(2) - at(1) * 2.0f + cv) * inv;
     return (cv - at(-1) * 2.0f + at(-2)) * inv;
 }
 
 // First derivative along one axis at offset (oi, oj, ok), one-sided first order at the faces
 // (QSR.cu:245-273). `pos` is the absolute coordinate of the offset cell along AX.
-template <int AX, class Acc>
+template <int AX, bool kFaces = true, class Acc>
 __device__ __forceinline__ float d1_face(const Acc& A, int c, int oi, int oj, int ok, int pos, int n, float i2, float i1) {
     auto at = [&](int s) {
         return AX == 0 ? A(c, oi + s, oj, ok) : (AX == 1 ? A(c, oi, oj + s, ok) : A(c, oi, oj, ok + s));
     };
-    if (pos > 0 && pos < n - 1) return (at(1) - at(-1)) * i2;
+    if (!kFaces || (pos > 0 && pos < n - 1)) return (at(1) - at(-1)) * i2;
     if (pos == 0) return (at(1) - at(0)) * i1;
     return (at(0) - at(-1)) * i1;
 }
 
 // Column divergence D_j = d_k Q_kj at offset (oi, oj, ok) of cell (i, j, k) (QSR.cu:325-371).
-template <class Acc>
+template <bool kFaces = true, class Acc>
 __device__ __forceinline__ void dcol_at(const Acc& A, const QsrConst& P, int i, int j, int k, int oi, int oj, int ok,
                                         float D[3]) {
     const int pi = i + oi, pj = j + oj, pk = k + ok;
-    D[0] = d1_face<0>(A, 0, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 1, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
-           d1_face<2>(A, 2, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
-    D[1] = d1_face<0>(A, 1, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 3, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
-           d1_face<2>(A, 4, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
-    D[2] = d1_face<0>(A, 2, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) + d1_face<1>(A, 4, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
-           d1_face<2>(A, 5, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+    D[0] = d1_face<0, kFaces>(A, 0, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) +
+           d1_face<1, kFaces>(A, 1, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2, kFaces>(A, 2, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+    D[1] = d1_face<0, kFaces>(A, 1, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) +
+           d1_face<1, kFaces>(A, 3, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2, kFaces>(A, 4, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
+    D[2] = d1_face<0, kFaces>(A, 2, oi, oj, ok, pi, P.Nx, P.i2x, P.ix) +
+           d1_face<1, kFaces>(A, 4, oi, oj, ok, pj, P.Ny, P.i2y, P.iy) +
+           d1_face<2, kFaces>(A, 5, oi, oj, ok, pk, P.Nz, P.i2z, P.iz);
 }
 
 // Bulk molecular field entries xx yy zz xy xz yz (QSR.cu:399-417).
@@ -168,14 +173,15 @@ __device__ __forceinline__ void surface_q0(const QsrConst& P, int i, int j, int 
 // then L3 on interior cells re-projected, then the weak-anchoring penalty
 // (QSR.cu:373-472, 474-621, 623-652). `lap` returns the Laplacian (IMEX uses it).
 // DAcc(c, di, dj, dk) returns the column divergence D_c at a face-neighbour offset.
-template <bool kL2, bool kL3, class Acc, class DAcc>
+// kFaces = false: the caller guarantees the cell and all stencil positions are interior.
+template <bool kL2, bool kL3, bool kFaces = true, class Acc, class DAcc>
 __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, const QsrConst& P, int i, int j, int k,
                                                const float q[5], bool anchor, float mu[5], float lap[5]) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-        const float d2x = d2_face<0>(A, c, q[c], i, P.Nx, P.ix2);
-        const float d2y = d2_face<1>(A, c, q[c], j, P.Ny, P.iy2);
-        const float d2z = d2_face<2>(A, c, q[c], k, P.Nz, P.iz2);
+        const float d2x = d2_face<0, kFaces>(A, c, q[c], i, P.Nx, P.ix2);
+        const float d2y = d2_face<1, kFaces>(A, c, q[c], j, P.Ny, P.iy2);
+        const float d2z = d2_face<2, kFaces>(A, c, q[c], k, P.Nz, P.iz2);
         lap[c] = d2x + d2y + d2z;
     }
     float h[6];
@@ -197,7 +203,7 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
             auto at = [&](int s) {
                 return ax == 0 ? DA(comp, s, 0, 0) : (ax == 1 ? DA(comp, 0, s, 0) : DA(comp, 0, 0, s));
             };
-            if (pos > 0 && pos < n - 1) return (at(1) - at(-1)) * i2;
+            if (!kFaces || (pos > 0 && pos < n - 1)) return (at(1) - at(-1)) * i2;
             if (pos == 0) return (at(1) - at(0)) * i1;
             return (at(0) - at(-1)) * i1;
         };
@@ -216,7 +222,8 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
     mu[3] = h[1] - corr;
     mu[4] = h[5];
     if (kL3) {
-        const bool interior = (i > 0 && i < P.Nx - 1 && j > 0 && j < P.Ny - 1 && k > 0 && k < P.Nz - 1);
+        const bool interior =
+            !kFaces || (i > 0 && i < P.Nx - 1 && j > 0 && j < P.Ny - 1 && k > 0 && k < P.Nz - 1);
         if (interior) {
             float hx[6] = {mu[0], mu[3], -(mu[0] + mu[3]), mu[1], mu[2], mu[4]};
             float d[6][3];
@@ -241,16 +248,19 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
             hx[5] += hl3 * M(1, 2);
             const float Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4], Qzz = -q[0] - q[3];
             const float Dc0 = DA(0, 0, 0, 0), Dc1 = DA(1, 0, 0, 0), Dc2 = DA(2, 0, 0, 0);
-            // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603).
+            // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603), with the Q_ab / (stencil
+            // denominator) weights formed once for all five components.
+            const float wxx = Qxx * P.ix2, wyy = Qyy * P.iy2, wzz = Qzz * P.iz2;
+            const float wxy = 2.0f * Qxy * P.i4xy, wxz = 2.0f * Qxz * P.i4xz, wyz = 2.0f * Qyz * P.i4yz;
             auto Bc = [&](int c) {
-                const float Qc = c == 5 ? Qzz : q[c];
-                const float d2xx = (A(c, 1, 0, 0) - 2.0f * Qc + A(c, -1, 0, 0)) * P.ix2;
-                const float d2yy = (A(c, 0, 1, 0) - 2.0f * Qc + A(c, 0, -1, 0)) * P.iy2;
-                const float d2zz = (A(c, 0, 0, 1) - 2.0f * Qc + A(c, 0, 0, -1)) * P.iz2;
-                const float d2xy = (A(c, 1, 1, 0) - A(c, 1, -1, 0) - A(c, -1, 1, 0) + A(c, -1, -1, 0)) * P.i4xy;
-                const float d2xz = (A(c, 1, 0, 1) - A(c, 1, 0, -1) - A(c, -1, 0, 1) + A(c, -1, 0, -1)) * P.i4xz;
-                const float d2yz = (A(c, 0, 1, 1) - A(c, 0, 1, -1) - A(c, 0, -1, 1) + A(c, 0, -1, -1)) * P.i4yz;
-                const float contract = Qxx * d2xx + Qyy * d2yy + Qzz * d2zz + 2.0f * (Qxy * d2xy + Qxz * d2xz + Qyz * d2yz);
+                const float Qc2 = 2.0f * (c == 5 ? Qzz : q[c]);
+                const float sxx = A(c, 1, 0, 0) - Qc2 + A(c, -1, 0, 0);
+                const float syy = A(c, 0, 1, 0) - Qc2 + A(c, 0, -1, 0);
+                const float szz = A(c, 0, 0, 1) - Qc2 + A(c, 0, 0, -1);
+                const float sxy = (A(c, 1, 1, 0) - A(c, 1, -1, 0)) - (A(c, -1, 1, 0) - A(c, -1, -1, 0));
+                const float sxz = (A(c, 1, 0, 1) - A(c, 1, 0, -1)) - (A(c, -1, 0, 1) - A(c, -1, 0, -1));
+                const float syz = (A(c, 0, 1, 1) - A(c, 0, 1, -1)) - (A(c, 0, -1, 1) - A(c, 0, -1, -1));
+                const float contract = wxx * sxx + wyy * syy + wzz * szz + wxy * sxy + wxz * sxz + wyz * syz;
                 return Dc0 * d[c][0] + Dc1 * d[c][1] + Dc2 * d[c][2] + contract;
             };
             const float Bxx = Bc(0), Byy = Bc(3), Bzz = -(Bxx + Byy);

@@ -168,12 +168,27 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     // Column divergence of plane p on the tile plus a 1-cell halo into D slot (p + 1) % 3.
     // Reads Q planes p-1 .. p+1 (all waited for by the caller).
+    // The tile plus its 2-cell halo lies strictly inside the grid in j and k: planes with
+    // 2 <= i <= Nx-3 then need no face stencils anywhere (cells, divergence halo, L3).
+    const bool tile_interior = (j0 >= 2) && (j0 + TJ + 2 <= P.Ny) && (k0 >= 2) && (k0 + TK + 2 <= P.Nz);
     auto compute_D = [&](int p) {
         if (p < 0 || p >= P.Nx) return;
         float* dst = sd + ((p + 1) % 3) * DPLANE;
         SmemQ A;
 #pragma unroll
         for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(p + d - 2, base)) * PLANE;
+        if (tile_interior && p >= 1 && p <= P.Nx - 2) {
+            for (int t = tid; t < DROWS * DRW; t += THREADS) {
+                const int r = t / DRW, cidx = t - r * DRW;
+                float D[3];
+                A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
+                dcol_at<false>(A, P, p, j0 + r - 1, k0 + cidx - 1, 0, 0, 0, D);
+                dst[t] = D[0];
+                dst[DCSTR + t] = D[1];
+                dst[2 * DCSTR + t] = D[2];
+            }
+            return;
+        }
         for (int t = tid; t < DROWS * DRW; t += THREADS) {
             const int r = t / DRW, cidx = t - r * DRW;
             const int j = j0 + r - 1, k = k0 + cidx - 1;
@@ -227,7 +242,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                     for (int d = 0; d < 3; ++d) DA.pl[d] = sd + ((i + d) % 3) * DPLANE;
                     DA.off = (jl + 1) * DRW + (kl + 1);
                     float mu[5], lap[5];
-                    chem_potential<kL2, kL3>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                    if (tile_interior && i >= 2 && i <= P.Nx - 3)
+                        chem_potential<kL2, kL3, false>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                    else
+                        chem_potential<kL2, kL3, true>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
                     const uint32_t cell = (uint32_t)(k + P.Nz * (j + P.Ny * i));
                     if (kRHS) {
 #pragma unroll
@@ -306,6 +324,9 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     using namespace tiled;
     plan = TiledPlan{};
     const int ntj = (Ny + TJ - 1) / TJ, ntk = (Nz + TK - 1) / TK;
+    // Planes per work item: CHUNK by default, LDG_QSR_CHUNK (8..4096) to tune.
+    int chunk = CHUNK;
+    if (const char* e = getenv("LDG_QSR_CHUNK")) chunk = std::min(4096, std::max(8, atoi(e)));
     std::vector<int4> items;
     long long active = 0, written = 0;
     for (int jt = 0; jt < ntj; ++jt)
@@ -327,8 +348,8 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
             const long long tile_cells = (long long)(std::min(Ny, (jt + 1) * TJ) - jt * TJ) *
                                          (std::min(Nz, (kt + 1) * TK) - kt * TK);
             active += tile_cells * (imax - imin + 1);
-            for (int i = imin; i <= imax; i += CHUNK)
-                items.push_back(make_int4(jt * TJ, kt * TK, i, std::min(imax + 1, i + CHUNK)));
+            for (int i = imin; i <= imax; i += chunk)
+                items.push_back(make_int4(jt * TJ, kt * TK, i, std::min(imax + 1, i + chunk)));
         }
     // `written` above counts cells per (row) once a row has one; recount exactly.
     written = 0;

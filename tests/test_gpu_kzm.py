@@ -67,3 +67,22 @@ def test_periodic_noise_statistics(oracle):
     s.upload(np.zeros(5 * 32 ** 3))
     s.step(1, 0.0, 1e6, 1e6, 1e-12, noise_sigma=sigma, seed=777, step_index=3)
     assert np.array_equal(s.download() / sigma, z)
+
+
+@pytest.mark.parametrize("shape", [(64, 40, 70), (33, 17, 9), (2, 3, 4), (32, 8, 32)])
+def test_tiled_periodic_kernel_matches_direct(oracle, shape, monkeypatch):
+    # the z-marching tiled kernel (default) and the one-thread-per-site kernel agree, with noise
+    A, B, C = bulk_ABC(0.044e6, 1.413e6, 1.153e6, 300.0, 307.0)
+    bp, s = _pair(*shape, dy=1.1e-8)
+    q0 = fp32(oracle.bulk_init(bp, 5, 0.05))
+    s.upload(q0)
+    s.step(6, A, B, C, bp.dt, noise_sigma=1e-4, seed=99, step_index=10)
+    tiled = s.download()
+    s.close()
+    monkeypatch.setenv("LDG_KZM_KERNEL", "direct")
+    bp, s2 = _pair(*shape, dy=1.1e-8)
+    s2.upload(q0)
+    s2.step(6, A, B, C, bp.dt, noise_sigma=1e-4, seed=99, step_index=10)
+    direct = s2.download()
+    s2.close()
+    assert rel_err(tiled, direct) <= 1e-6
