@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) k_kzm_step(const float* __restrict__ q, f
     h[3] -= P.kappa * lap[1];
     h[4] -= P.kappa * lap[2];
     h[5] -= P.kappa * lap[4];
-    const float corr = (h[0] + h[1] + h[2]) / 3.0f;
+    const float corr = (h[0] + h[1] + h[2]) * (1.0f / 3.0f);
     float u[5] = {c[0] - P.mob_dt * (h[0] - corr), c[1] - P.mob_dt * h[3], c[2] - P.mob_dt * h[4],
                   c[3] - P.mob_dt * (h[1] - corr), c[4] - P.mob_dt * h[5]};
     if (kNoise) {
@@ -109,7 +109,8 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_tiled(const float* __rest
     const long long rowm = (long long)((y0 + P.Ny - 1) % P.Ny) * P.sy;   // halo row y0-1
     const long long rowp = (long long)((y0 + KTY) % P.Ny) * P.sy;        // halo row y0+KTY
     const int xm = (x0 + P.Nx - 1) % P.Nx, xp = (x0 + KTX) % P.Nx;       // halo columns
-    auto zw = [&](int z) { return (z % P.Nz + P.Nz) % P.Nz; };
+    // z stays within [-1, 2 Nz) here (Nz >= 2), so one compare-and-add wraps it.
+    auto zw = [&](int z) { return z < 0 ? z + P.Nz : (z >= P.Nz ? z - P.Nz : z); };
     auto load5 = [&](int z, float v[5]) {
         const long long o = (long long)zw(z) * P.sz + row + x;
 #pragma unroll
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_tiled(const float* __rest
             h[3] -= P.kappa * lap[1];
             h[4] -= P.kappa * lap[2];
             h[5] -= P.kappa * lap[4];
-            const float corr = (h[0] + h[1] + h[2]) / 3.0f;
+            const float corr = (h[0] + h[1] + h[2]) * (1.0f / 3.0f);
             float u[5] = {qc[0] - P.mob_dt * (h[0] - corr), qc[1] - P.mob_dt * h[3], qc[2] - P.mob_dt * h[4],
                           qc[3] - P.mob_dt * (h[1] - corr), qc[4] - P.mob_dt * h[5]};
             if (kNoise) {
@@ -191,6 +192,116 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_tiled(const float* __rest
             qn[m] = qn2[m];
         }
     }
+}
+
+// Asynchronous-copy variant: every plane of the tile plus its periodically wrapped halo is
+// fetched with cp.async (4-byte copies, any wrapped address) into a 5-plane shared ring two
+// planes ahead of use, so no thread waits on a global load inside the plane loop; x, y and z
+// neighbours all come from shared memory; one CTA barrier per plane.
+constexpr int KRING = 5;
+constexpr int KPS = (KTY + 2) * (KTX + 2);  // floats per component plane of the ring
+__device__ __forceinline__ void cp_async4(float* sdst, const float* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <bool kNoise>
+__global__ void __launch_bounds__(KTX* KTY) k_kzm_step_async(const float* __restrict__ q, float* __restrict__ out,
+                                                             KzmConst P) {
+    extern __shared__ __align__(16) float ring[];  // [KRING][5][KTY+2][KTX+2]
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * KTX, y0 = blockIdx.y * KTY, z0 = blockIdx.z * KZC;
+    const int z1 = min(z0 + KZC, P.Nz);
+    const int xr = x0 + tx, yr = y0 + ty;
+    const bool valid = (xr < P.Nx) && (yr < P.Ny);
+    const int x = xr % P.Nx, y = yr % P.Ny;
+    const long long g_c = (long long)y * P.sy + x;
+    const int s_c = (ty + 1) * (KTX + 2) + tx + 1;
+    // Flat copy list: the 5 x (KTY+2) x (KTX+2) ring entries of a plane spread over the CTA's
+    // threads; each thread's (global in-plane offset, shared offset) pairs are the same for every
+    // plane, so they are formed once here (wrapped periodically).
+    constexpr int NE = 5 * KPS;
+    constexpr int PER = (NE + KTX * KTY - 1) / (KTX * KTY);
+    const int tid = ty * KTX + tx;
+    long long goff[PER];
+    int soff[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int e = tid + t * KTX * KTY;
+        const int m = e / KPS, cell = e - m * KPS;
+        const int r = cell / (KTX + 2), cc = cell - r * (KTX + 2);
+        const int gx = (x0 - 1 + cc + P.Nx) % P.Nx, gy = (y0 - 1 + r + P.Ny) % P.Ny;
+        goff[t] = (long long)min(m, 4) * P.sc + (long long)gy * P.sy + gx;
+        soff[t] = e;
+    }
+    auto zw = [&](int z) { return z < 0 ? z + P.Nz : (z >= P.Nz ? z - P.Nz : z); };
+    auto issue = [&](int p) {
+        float* dst = ring + ((p + KRING) % KRING) * NE;
+        const float* src = q + (long long)zw(p) * P.sz;
+#pragma unroll
+        for (int t = 0; t < PER; ++t)
+            if (t < PER - 1 || soff[t] < NE) cp_async4(dst + soff[t], src + goff[t]);
+    };
+    // Prologue: planes z0-1 .. z0+2, one commit group each.
+    for (int p = z0 - 1; p <= z0 + 2; ++p) {
+        issue(p);
+        cp_async_commit();
+    }
+    const uint32_t cell_base = (uint32_t)(x + P.Nx * y);
+    for (int z = z0; z < z1; ++z) {
+        cp_async_wait<1>();  // all groups but the newest (plane z+2): planes z-1 .. z+1 are in
+        __syncthreads();     // every thread's copies visible; every thread done with plane z-2
+        if (z + 3 <= z1) issue(z + 3);  // into the slot of plane z-2
+        cp_async_commit();
+        if (valid) {
+            const float* pm = ring + ((z - 1 + KRING) % KRING) * 5 * KPS;
+            const float* pc = ring + ((z + KRING) % KRING) * 5 * KPS;
+            const float* pp = ring + ((z + 1) % KRING) * 5 * KPS;
+            float c[5], lap[5];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                const float* s = pc + m * KPS + s_c;
+                c[m] = s[0];
+                lap[m] = (s[1] - 2.0f * c[m] + s[-1]) * P.ix2 + (s[KTX + 2] - 2.0f * c[m] + s[-(KTX + 2)]) * P.iy2 +
+                         (pp[m * KPS + s_c] - 2.0f * c[m] + pm[m * KPS + s_c]) * P.iz2;
+            }
+            float h[6];
+            bulk_field(c, P.A, P.B, P.C, h);
+            h[0] -= P.kappa * lap[0];
+            h[1] -= P.kappa * lap[3];
+            h[2] += P.kappa * (lap[0] + lap[3]);
+            h[3] -= P.kappa * lap[1];
+            h[4] -= P.kappa * lap[2];
+            h[5] -= P.kappa * lap[4];
+            const float corr = (h[0] + h[1] + h[2]) * (1.0f / 3.0f);
+            float u[5] = {c[0] - P.mob_dt * (h[0] - corr), c[1] - P.mob_dt * h[3], c[2] - P.mob_dt * h[4],
+                          c[3] - P.mob_dt * (h[1] - corr), c[4] - P.mob_dt * h[5]};
+            if (kNoise) {
+                float g[5];
+                normals5(cell_base + (uint32_t)P.Nx * (uint32_t)P.Ny * (uint32_t)z, 0u, P.step, P.key0, P.key1, g);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) u[m] += P.sigma * g[m];
+            }
+            if (P.qcap > 0.0f) {
+                const float zz = -u[0] - u[3];
+                const float tr = u[0] * u[0] + u[3] * u[3] + zz * zz + 2.0f * (u[1] * u[1] + u[2] * u[2] + u[4] * u[4]);
+                const float qn_ = sqrtf(fmaxf(tr, 0.0f));
+                if (qn_ > P.qcap && qn_ > 0.0f) {
+                    const float sc = P.qcap / qn_;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) u[m] *= sc;
+                }
+            }
+            float* o = out + (long long)z * P.sz + g_c;
+#pragma unroll
+            for (int m = 0; m < 5; ++m) o[m * P.sc] = u[m];
+        }
+    }
+    cp_async_wait<0>();  // no copy into this CTA's shared memory outlives it
 }
 
 __global__ void k_kzm_from_aos(const double* __restrict__ aos, float* __restrict__ a, KzmConst P) {
@@ -590,19 +701,26 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
     P.sigma = (float)a->noise_sigma;
     P.key0 = (uint32_t)a->seed;
     P.key1 = (uint32_t)(a->seed >> 32);
-    // Tiled z-marching kernel by default; LDG_KZM_KERNEL=direct selects the one-thread-per-site kernel.
+    // Asynchronous-copy tiled kernel by default; LDG_KZM_KERNEL=direct selects the one-thread-per-
+    // site kernel, LDG_KZM_KERNEL=regs the register-queue tiled kernel.
     const char* ksel = getenv("LDG_KZM_KERNEL");
-    const bool direct = ksel && std::strcmp(ksel, "direct") == 0;
+    const int kind = (ksel && std::strcmp(ksel, "direct") == 0) ? 0 : ((ksel && std::strcmp(ksel, "regs") == 0) ? 1 : 2);
     dim3 blk(32, 8, 1), grd((P.Nx + 31) / 32, (P.Ny + 7) / 8, P.Nz);
     dim3 tgrd((P.Nx + KTX - 1) / KTX, (P.Ny + KTY - 1) / KTY, (P.Nz + KZC - 1) / KZC);
+    const size_t ring_bytes = (size_t)KRING * 5 * KPS * sizeof(float);
     for (int s = 0; s < n_steps; ++s) {
         P.step = a->step_index + s;
         const bool noise = a->noise_sigma > 0.0;
-        if (!direct) {
-            if (noise) k_kzm_step_tiled<true><<<tgrd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
-            else k_kzm_step_tiled<false><<<tgrd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
-        } else if (noise) k_kzm_step<true><<<grd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
-        else k_kzm_step<false><<<grd, blk, 0, h->stream>>>(h->q[h->cur], h->q[1 - h->cur], P);
+        const float* in = h->q[h->cur];
+        float* outb = h->q[1 - h->cur];
+        if (kind == 2) {
+            if (noise) k_kzm_step_async<true><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
+            else k_kzm_step_async<false><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
+        } else if (kind == 1) {
+            if (noise) k_kzm_step_tiled<true><<<tgrd, blk, 0, h->stream>>>(in, outb, P);
+            else k_kzm_step_tiled<false><<<tgrd, blk, 0, h->stream>>>(in, outb, P);
+        } else if (noise) k_kzm_step<true><<<grd, blk, 0, h->stream>>>(in, outb, P);
+        else k_kzm_step<false><<<grd, blk, 0, h->stream>>>(in, outb, P);
         h->launches++;
         LDG_LAUNCHED("k_kzm_step");
         h->cur = 1 - h->cur;

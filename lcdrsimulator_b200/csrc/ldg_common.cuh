@@ -65,28 +65,32 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
     }
 }
 
-// Uniform in (0, 1] from the top 24 bits.
-__device__ __forceinline__ float u01(uint32_t x) { return ((float)(x >> 8) + 1.0f) * (1.0f / 16777216.0f); }
+// Uniform in (0, 1] from a 21-bit integer.
+__device__ __forceinline__ float u21(uint32_t x) { return ((float)x + 1.0f) * (1.0f / 2097152.0f); }
 
-// Five standard normals for (cell, instance, step): two Philox blocks, Box-Muller pairs.
+// Five standard normals for (cell, instance, step) from one Philox4x32-10 block: the four
+// 32-bit words give six disjoint 21-bit fields (the low 21 bits of each word, and the high
+// 11 bits of words 0|1 and 2|3 joined), i.e. three Box-Muller pairs; the sixth normal is
+// not needed. Counter = (cell, instance, step low word, step high word).
 __device__ __forceinline__ void normals5(uint32_t cell, uint32_t instance, long long step, uint32_t k0, uint32_t k1,
                                          float g[5]) {
-    float z[8];
-#pragma unroll
-    for (int blk = 0; blk < 2; ++blk) {
-        uint32_t c[4] = {cell, instance, (uint32_t)step, ((uint32_t)((unsigned long long)step >> 32) << 1) | (uint32_t)blk};
-        philox4x32_10(c, k0, k1);
-#pragma unroll
-        for (int p = 0; p < 2; ++p) {
-            const float r = sqrtf(-2.0f * logf(u01(c[2 * p])));
-            float s, co;
-            sincospif(2.0f * u01(c[2 * p + 1]), &s, &co);
-            z[4 * blk + 2 * p] = r * co;
-            z[4 * blk + 2 * p + 1] = r * s;
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < 5; ++m) g[m] = z[m];
+    uint32_t c[4] = {cell, instance, (uint32_t)step, (uint32_t)((unsigned long long)step >> 32)};
+    philox4x32_10(c, k0, k1);
+    constexpr uint32_t M21 = (1u << 21) - 1u;
+    const uint32_t f0 = c[0] & M21, f1 = c[1] & M21, f2 = c[2] & M21, f3 = c[3] & M21;
+    const uint32_t f4 = ((c[0] >> 21) << 10) | (c[1] >> 22);  // 11 + 10 bits
+    const uint32_t f5 = ((c[2] >> 21) << 10) | (c[3] >> 22);
+    float s, co;
+    float r = sqrtf(-2.0f * logf(u21(f0)));
+    sincospif(2.0f * u21(f1), &s, &co);
+    g[0] = r * co;
+    g[1] = r * s;
+    r = sqrtf(-2.0f * logf(u21(f2)));
+    sincospif(2.0f * u21(f3), &s, &co);
+    g[2] = r * co;
+    g[3] = r * s;
+    r = sqrtf(-2.0f * logf(u21(f4)));
+    g[4] = r * cospif(2.0f * u21(f5));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -145,7 +149,7 @@ __device__ __forceinline__ void bulk_field(const float q[5], float cQ, float cQ2
     const float q2yy = Qxy * Qxy + Qyy * Qyy + Qyz * Qyz;
     const float q2yz = Qxy * Qxz + Qyy * Qyz + Qyz * Qzz;
     const float q2zz = Qxz * Qxz + Qyz * Qyz + Qzz * Qzz;
-    const float t3 = trQ2 / 3.0f;
+    const float t3 = trQ2 * (1.0f / 3.0f);  // FP32 path: reciprocal multiply (one rounding)
     const float g = cQ3 * trQ2;
     h[0] = cQ * Qxx - cQ2 * (q2xx - t3) + g * Qxx;
     h[1] = cQ * Qyy - cQ2 * (q2yy - t3) + g * Qyy;
@@ -215,7 +219,7 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
         h[4] -= L2 * (dD(2, 0) + dD(0, 2));
         h[5] -= L2 * (dD(2, 1) + dD(1, 2));
     }
-    float corr = (h[0] + h[1] + h[2]) / 3.0f;
+    float corr = (h[0] + h[1] + h[2]) * (1.0f / 3.0f);
     mu[0] = h[0] - corr;
     mu[1] = h[3];
     mu[2] = h[4];
@@ -271,7 +275,7 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
             hx[3] -= P.L3 * Bxy;
             hx[4] -= P.L3 * Bxz;
             hx[5] -= P.L3 * Byz;
-            corr = (hx[0] + hx[1] + hx[2]) / 3.0f;
+            corr = (hx[0] + hx[1] + hx[2]) * (1.0f / 3.0f);
             mu[0] = hx[0] - corr;
             mu[3] = hx[1] - corr;
             mu[1] = hx[3];

@@ -4,9 +4,9 @@
 // of planes. Each plane of the input field arrives in shared memory through one TMA load
 // of a 4-D box (k, j, i, component) covering the tile plus a halo of 2 rows and 4 columns
 // (the k start stays on a 16-byte boundary), so every Q value is read from HBM about once.
-// The ring holds the planes i-2 .. i+2 plus PF planes in flight. The column divergence D
-// (needed by the L2 and L3 terms) is computed once per plane on the tile plus a 1-cell halo
-// into a 3-plane shared ring. Per cell the kernel then evaluates the chemical potential and
+// The ring holds the planes i-2 .. i+3 plus the planes in flight. The column divergence D
+// (needed by the L2 and L3 terms) is computed once per plane, one plane ahead, on the tile
+// plus a 1-cell halo into a 4-plane shared ring, so each plane costs one CTA barrier. Per cell the kernel then evaluates the chemical potential and
 // the update from shared memory and writes only the cells that change (moving and strongly
 // anchored cells): frozen exterior cells hold identical values in both ping-pong buffers.
 // Tiles that contain no changing cell are never visited (host-built work list).
@@ -39,11 +39,11 @@ constexpr int RW = TK + 2 * HK;      // 40 floats per smem row
 constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
 constexpr int CSTR = RW * ROWS;      // floats per component plane
 constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
-constexpr int PF = 2;                // planes in flight beyond i+2
-constexpr int NQ = 5 + PF;           // ring slots
+constexpr int NQ = 8;                // Q ring slots: planes i-2 .. i+3 in use, the rest in flight
 constexpr int DRW = TK + 2, DROWS = TJ + 2;
 constexpr int DCSTR = DRW * DROWS;
 constexpr int DPLANE = 3 * DCSTR;
+constexpr int NDS = 4;               // D ring slots: D(i-1) .. D(i+2)
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
 constexpr int CHUNK = 32;            // planes per work item
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
@@ -121,7 +121,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* sq = reinterpret_cast<float*>(smem_raw);
     float* sd = sq + NQ * PLANE;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sd + (kD ? 3 * DPLANE : 0));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sd + (kD ? NDS * DPLANE : 0));
+    // Plane lookahead: with the divergence, step i computes D(i+2), which reads Q(i+3).
+    constexpr int LOOK = kD ? 3 : 2;
     int* s_abort = reinterpret_cast<int*>(bar + NQ);
 
     const int4 item = items[blockIdx.x];
@@ -166,14 +168,14 @@ __global__ void __launch_bounds__(THREADS, 1)
         waited_end = p + 1;
     };
 
-    // Column divergence of plane p on the tile plus a 1-cell halo into D slot (p + 1) % 3.
+    // Column divergence of plane p on the tile plus a 1-cell halo into D slot (p + 4) % 4.
     // Reads Q planes p-1 .. p+1 (all waited for by the caller).
     // The tile plus its 2-cell halo lies strictly inside the grid in j and k: planes with
     // 2 <= i <= Nx-3 then need no face stencils anywhere (cells, divergence halo, L3).
     const bool tile_interior = (j0 >= 2) && (j0 + TJ + 2 <= P.Ny) && (k0 >= 2) && (k0 + TK + 2 <= P.Nz);
     auto compute_D = [&](int p) {
         if (p < 0 || p >= P.Nx) return;
-        float* dst = sd + ((p + 1) % 3) * DPLANE;
+        float* dst = sd + ((p + NDS) % NDS) * DPLANE;
         SmemQ A;
 #pragma unroll
         for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(p + d - 2, base)) * PLANE;
@@ -203,24 +205,24 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     };
 
-    // Prologue: planes ib-2 .. ib+1, then D(ib-1) and D(ib).
-    for (int p = base; p <= ib + 1; ++p) wait_plane(p);
+    // Prologue: planes ib-2 .. ib+LOOK-1, then D(ib-1) .. D(ib+1) (visible after the barrier).
+    for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     __syncthreads();
     if (kD && !*s_abort) {
         compute_D(ib - 1);
         compute_D(ib);
+        compute_D(ib + 1);
     }
+    __syncthreads();
 
     const int j = j0 + jl, k = k0 + kl;
     const bool in_grid = (j < P.Ny) && (k < P.Nz);
+    // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
+    // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
     for (int i = ib; i < ie; ++i) {
-        wait_plane(i + 2);
-        __syncthreads();
-        if (*s_abort) break;
-        if (kD) {
-            compute_D(i + 1);
-            __syncthreads();
-        }
+        if (*s_abort) break;  // uniform: read after a barrier
+        wait_plane(i + LOOK);
+        if (kD) compute_D(i + 2);
         if (in_grid) {
             const long long id = (long long)i * P.si + (long long)j * P.sj + k;
             const uint8_t f = __ldg(flags + id);
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 } else {
                     SmemD DA;
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) DA.pl[d] = sd + ((i + d) % 3) * DPLANE;
+                    for (int d = 0; d < 3; ++d) DA.pl[d] = sd + ((i + d - 1 + NDS) % NDS) * DPLANE;
                     DA.off = (jl + 1) * DRW + (kl + 1);
                     float mu[5], lap[5];
                     if (tile_interior && i >= 2 && i <= P.Nx - 3)
@@ -380,7 +382,7 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     plan.bufs[0] = buf0;
     plan.bufs[1] = buf1;
     plan.smem_bytes[0] = (size_t)NQ * PLANE * 4 + NQ * 8 + 16;
-    plan.smem_bytes[1] = (size_t)NQ * PLANE * 4 + (size_t)3 * DPLANE * 4 + NQ * 8 + 16;
+    plan.smem_bytes[1] = (size_t)NQ * PLANE * 4 + (size_t)NDS * DPLANE * 4 + NQ * 8 + 16;
     plan.ok = true;
     return LDG_OK;
 }

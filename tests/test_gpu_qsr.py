@@ -141,16 +141,17 @@ def test_noise_stream_matches_philox_box_muller(oracle):
     move = (fl & 2) != 0  # evolving cells (ORC_EVOLVE with W > 0)
     k0, k1 = seed & 0xFFFFFFFF, seed >> 32
     idx = np.flatnonzero(move)
+    m21 = (1 << 21) - 1
     for cell in idx[:: max(1, len(idx) // 40)]:
-        z = []
-        for blk in range(2):
-            w = oracle.philox([int(cell), 0, step & 0xFFFFFFFF, ((step >> 32) << 1) | blk], [k0, k1])
-            for p in range(2):
-                u1 = ((w[2 * p] >> 8) + 1.0) / 16777216.0
-                u2 = ((w[2 * p + 1] >> 8) + 1.0) / 16777216.0
-                r = math.sqrt(-2.0 * math.log(u1))
-                z += [r * math.cos(2 * math.pi * u2), r * math.sin(2 * math.pi * u2)]
-        assert np.allclose(got[cell], sigma * np.array(z[:5]), rtol=2e-5, atol=1e-5 * sigma)
+        w = oracle.philox([int(cell), 0, step & 0xFFFFFFFF, step >> 32], [k0, k1])
+        f = [w[0] & m21, w[1] & m21, w[2] & m21, w[3] & m21, ((w[0] >> 21) << 10) | (w[1] >> 22),
+             ((w[2] >> 21) << 10) | (w[3] >> 22)]
+        u = [(x + 1.0) / 2097152.0 for x in f]
+        r = [math.sqrt(-2.0 * math.log(u[0])), math.sqrt(-2.0 * math.log(u[2])), math.sqrt(-2.0 * math.log(u[4]))]
+        z = [r[0] * math.cos(2 * math.pi * u[1]), r[0] * math.sin(2 * math.pi * u[1]),
+             r[1] * math.cos(2 * math.pi * u[3]), r[1] * math.sin(2 * math.pi * u[3]),
+             r[2] * math.cos(2 * math.pi * u[5])]
+        assert np.allclose(got[cell], sigma * np.array(z), rtol=2e-5, atol=1e-5 * sigma)
     assert np.all(got[~move] == 0.0)
     # distribution: zero mean, unit variance over all evolving cells and components
     zs = got[move].ravel() / sigma

@@ -1,0 +1,246 @@
+"""The drop-in host programs qsr_b200 and kzm_bulk_ldg_b200.
+
+CPU tests: config parsing semantics of the reference (QSR.cu:1195-1253) through --dry-run,
+CLI behaviour and input validation. GPU tests: full runs whose field files are compared
+with the FP64 oracle run on the same inputs (file precision %.6e for QSR, 16 digits for KZM).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "lcdrsimulator_b200", "_lib")
+QSR = os.path.join(LIB, "qsr_b200")
+KZM = os.path.join(LIB, "kzm_bulk_ldg_b200")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built(lib):
+    assert os.path.exists(QSR) and os.path.exists(KZM)
+
+
+def run(exe, cfg_text, tmp_path, *extra):
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text(cfg_text)
+    return subprocess.run([exe, "--config", str(cfg), *extra], cwd=tmp_path, capture_output=True, text=True,
+                          timeout=600)
+
+
+def resolved(out):
+    d = {}
+    for line in out.splitlines():
+        if line.startswith("resolved "):
+            k, v = line[len("resolved "):].split("=", 1)
+            d[k] = v
+    return d
+
+
+def test_help_and_missing_config(tmp_path):
+    r = subprocess.run([QSR, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--config" in r.stdout
+    r = subprocess.run([QSR], capture_output=True, text=True)
+    assert r.returncode == 2
+    r = subprocess.run([KZM, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0
+
+
+def test_config_semantics_dry_run(tmp_path):
+    text = """
+# comment line
+Nx = 32   # trailing comment
+Nx = 48
+Ny = 3.2e1
+Nz = 4e1
+init_mode = 7
+random_seed = 1e3
+L1 = 6e-12
+L2 = 3e-12
+xi_guard_enabled = off
+W = not_a_number
+boundary_order_mode = Custom
+boundary_S = 0.6
+no_equals_sign_here
+"""
+    r = run(QSR, text, tmp_path, "--dry-run")
+    assert r.returncode == 0, r.stdout + r.stderr
+    d = resolved(r.stdout)
+    assert d["grid"] == "48x32x40"          # last key wins; integers from float text
+    assert d["init_mode"] == "2"            # clamped to [0, 2]
+    assert d["random_seed"] == "1000"
+    assert float(d["kappa"]) == 0.0         # any L != 0 disables kappa
+    assert float(d["W"]) == 0.0             # unparsable -> default
+    assert float(d["S_shell"]) == 0.6       # custom policy (case-insensitive)
+
+
+def test_frank_mapping_dry_run(tmp_path):
+    r = run(QSR, "use_frank_map = yes\nK1 = 6e-12\nK2 = 4e-12\nK3 = 8e-12\nS_ref = 0.5\nxi_guard_enabled = n\n",
+            tmp_path, "--dry-run")
+    d = resolved(r.stdout)
+    S2, S3 = 0.25, 0.125
+    assert float(d["L2"]) == pytest.approx((6e-12 - 4e-12) / S2)
+    assert float(d["L3"]) == pytest.approx(9 / 4 * (8e-12 - 6e-12) / S3)
+    assert float(d["L1"]) == pytest.approx((6e-12 + 4e-12 - 8e-12) / (2 * S2))
+
+
+def test_guards_exit_codes_without_gpu(tmp_path):
+    # unstable elastic constants abort with exit 1 (QSR.cu:2071-2091)
+    r = run(QSR, "L1 = -1e-12\nL2 = 0\nxi_guard_enabled = n\n", tmp_path, "--dry-run")
+    assert r.returncode == 1
+    # xi guard enabled by default aborts an under-resolved run (QSR.cu:2102-2111)
+    r = run(QSR, "T = 300\nT_star = 307\nL1 = 6e-12\ndx = 1e-8\ndy = 1e-8\ndz = 1e-8\n", tmp_path, "--dry-run")
+    assert r.returncode == 1 and "correlation-length" in r.stdout
+    # KZM validation messages (KZM_bulk_ldg.cu:824-841)
+    r = run(KZM, "Nx = 1\n", tmp_path)
+    assert r.returncode == 1 and "KZM_bulk_ldg_cuda ERROR: Nx, Ny, and Nz must all be greater than 1" in r.stderr
+    r = run(KZM, "total_iters = 10\npre_equil_iters = 5\nramp_iters = 10\n", tmp_path)
+    assert r.returncode == 1 and "total_iters must be at least" in r.stderr
+
+
+def read_qtensor(path, n):
+    a = np.loadtxt(path)
+    assert a.shape == (n, 12)
+    return np.stack([a[:, 3], a[:, 4], a[:, 5], a[:, 7], a[:, 8]], axis=1).ravel()
+
+
+@pytest.mark.gpu
+def test_qsr_single_temperature_run_matches_oracle(tmp_path, oracle):
+    from oracle.oracle import make_params
+    cfg = """sim_mode = 1
+init_mode = 0
+random_seed = 42
+S0 = 0.5
+Nx = 24
+Ny = 24
+Nz = 24
+T = 302
+T_star = 307
+L1 = 6e-12
+L2 = 3e-12
+L3 = 1e-12
+W = 1e-5
+boundary_order_mode = custom
+boundary_S = 0.6
+xi_guard_enabled = n
+iterations = 60
+print_freq = 20
+dt = 1.5e-10
+console_output = n
+"""
+    r = run(QSR, cfg, tmp_path)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    log = (tmp_path / "free_energy_vs_iteration.dat").read_text().splitlines()
+    assert log[0] == ("iteration,bulk,elastic,anchoring,total,radiality,time,avg_S,max_S,"
+                      "defect_density_per_plaquette,defect_plaquettes_used,xi_grad_proxy,xi_grad_edges_used")
+    assert [int(l.split(",")[0]) for l in log[1:]] == [0, 20, 40]
+    assert (tmp_path / "output" / "nematic_field_iter_40.dat").exists()
+    q = read_qtensor(tmp_path / "Qtensor_output_final.dat", 24 ** 3)
+    op = make_params(Nx=24, Ny=24, Nz=24, T_star=307.0, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5)
+    g, fl = oracle.geometry(op)
+    q0 = oracle.init(op, g, 0, 42, 0.5)
+    want = oracle.step_explicit(op, g, fl, np.asarray(q0, np.float32).astype(np.float64), 302.0, 0.6, 1.5e-10, n=60)
+    assert np.abs(q - want).max() <= 1e-5 * np.abs(want).max()
+    # energy column vs the oracle at iteration 40 is covered by the library tests; here the
+    # log must be finite and the total the sum of its parts
+    last = [float(x) for x in log[-1].split(",")]
+    assert abs(last[4] - (last[1] + last[2] + last[3])) <= 1e-5 * abs(last[4])
+
+
+@pytest.mark.gpu
+def test_qsr_quench_instability_guard_aborts(tmp_path):
+    cfg = """sim_mode = 3
+init_mode = 0
+random_seed = 3
+Nx = 16
+Ny = 16
+Nz = 16
+T = 300
+T_star = 307
+L1 = 6e-12
+xi_guard_enabled = n
+use_semi_implicit = n
+total_iters = 50
+logFreq = 10
+snapshot_mode = 0
+S_abort = 0.01
+console_output = n
+out_dir = qout
+"""
+    r = run(QSR, cfg, tmp_path)
+    assert r.returncode == 1
+    assert "InstabilityGuard" in r.stderr
+    assert (tmp_path / "qout" / "quench_log.dat").exists()
+    assert not (tmp_path / "qout" / "Qtensor_output_final.dat").exists()
+
+
+@pytest.mark.gpu
+def test_qsr_quench_with_imex_and_noise_runs(tmp_path):
+    cfg = """sim_mode = 3
+init_mode = 2
+noise_amplitude = 1e-3
+random_seed = 7
+Nx = 24
+Ny = 24
+Nz = 24
+T_star = 307
+L1 = 6e-12
+xi_guard_enabled = n
+T_high = 315
+T_low = 295
+ramp_iters = 40
+total_iters = 60
+logFreq = 20
+snapshot_mode = 1
+snapshotFreq = 30
+noise_strength = 4.14
+console_output = n
+out_dir = q
+"""
+    r = run(QSR, cfg, tmp_path)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    log = (tmp_path / "q" / "quench_log.dat").read_text().splitlines()
+    assert log[0].startswith("iteration,time_s,dt_s,T_K,bulk")
+    assert [int(l.split(",")[0]) for l in log[1:]] == [0, 20, 40, 59]
+    for name in ("nematic_field_iter_0.dat", "nematic_field_iter_30.dat", "nematic_field_final.dat",
+                 "Qtensor_output_final.dat"):
+        assert (tmp_path / "q" / name).exists(), name
+
+
+@pytest.mark.gpu
+def test_kzm_run_matches_oracle(tmp_path, oracle):
+    from oracle.oracle import OrcBulkParams
+    cfg = """Nx = 16
+Ny = 12
+Nz = 10
+dx = 1e-8
+dy = 1e-8
+dz = 1e-8
+kappa = 6e-12
+gamma = 0.1
+T_star = 307
+T_high = 300
+T_low = 300
+pre_equil_iters = 0
+ramp_iters = 0
+total_iters = 30
+dt = 1e-10
+init_noise_amplitude = 0.05
+random_seed = 12345
+logFreq = 10
+out_dir = kz
+"""
+    r = run(KZM, cfg, tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    log = (tmp_path / "kz" / "quench_log.dat").read_text().splitlines()
+    assert log[0] == ("iteration,time_s,T_K,dt_s,bulk,elastic,anchoring,total,radiality,avg_S,max_S,"
+                      "defect_density_per_plaquette,defect_plaquettes_used,xi_grad_proxy,defect_line_density")
+    assert [int(l.split(",")[0]) for l in log[1:]] == [0, 10, 20, 30]
+    a = np.loadtxt(tmp_path / "kz" / "q_tensor_final.dat")
+    got = a[:, 3:8].ravel()
+    bp = OrcBulkParams(16, 12, 10, 1e-8, 1e-8, 1e-8, 6e-12, 0.1, 1e-10, 0.0, 0.1, 0.25)
+    q0 = np.asarray(oracle.bulk_init(bp, 12345, 0.05), np.float32).astype(np.float64)
+    A, B, C = oracle.bulk_ABC(0.044e6, 1.413e6, 1.153e6, 300.0, 307.0, 1)
+    want = oracle.bulk_step(bp, q0, A, B, C, n=30)
+    assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max()
+    assert (tmp_path / "kz" / "run_summary.txt").read_text().startswith("Nx=16\nNy=12\nNz=10\n")
