@@ -128,6 +128,59 @@ long long qsr_launch_count(const qsr_handle* h);
 int qsr_destroy(qsr_handle* h);
 
 /* ------------------------------------------------------------------------------------
+ * Ensemble of independent droplets (Kibble-Zurek statistics)
+ *
+ * Replaces the reference's process-level batching: its tools launch one QSR_cuda process per
+ * configuration, one after another (tools/quench_rate_sweep.py:530-537, 664-677). Here all
+ * instances advance together: every step is one persistent, work-stealing kernel launch over
+ * the active tiles of all instances; K steps are captured once as a CUDA graph and replayed.
+ * The step index lives on the device, so each instance's temperature protocol (QSR.cu:
+ * 2679-2687), shell order and Philox noise counter are evaluated in the kernel.
+ * ------------------------------------------------------------------------------------ */
+typedef struct ens_params {
+    double dx, dy, dz;
+    double a, b, c, T_star;
+    int bulk_modechoice;
+    double kappa, L1, L2, L3, W, gamma;
+    double dt, q_norm_cap;
+    int boundary_custom;            /* 1: S_shell = boundary_S, 0: S_eq(T) of each step       */
+    double boundary_S;
+    int protocol;                   /* 1 step quench, 2 linear ramp (QSR.cu:2437-2447)         */
+} ens_params;
+
+typedef struct ens_instance {
+    int N;                          /* cubic grid edge (cells)                                 */
+    double droplet_radius_cells;
+    double T_high, T_low;
+    long long pre_equil_iters, ramp_iters;
+    unsigned long long seed;        /* Philox key of the instance's noise                      */
+    double noise_sigma;             /* per-component Langevin amplitude (0 = off)              */
+} ens_instance;
+
+typedef struct ens_handle ens_handle;
+
+int ens_create(const ens_params* params, int n_instances, const ens_instance* instances, ens_handle** out);
+/* Reference initialisation per instance (QSR.cu:1834-1904) with random_seed = instance seed. */
+int ens_initial_fields(ens_handle* h, int init_mode, double S0, double noise_amplitude);
+int ens_upload(ens_handle* h, int instance, const double* q_aos5);
+int ens_download(ens_handle* h, int instance, double* q_aos5);
+/* Advances every instance by n_steps (replays a captured CUDA graph of n_steps launches). */
+int ens_step(ens_handle* h, int n_steps);
+/* Observables of one instance at the current step; args NULL: T and S_shell from the
+ * instance's protocol, slices Nz/2, thresholds 0.1 / 0.25. */
+int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_observables* out);
+long long ens_step_index(const ens_handle* h);
+/* Times each candidate work-item length (planes per tile item) for trial_steps steps and keeps
+ * the fastest; the fields and the step index are restored afterwards. */
+int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk);
+long long ens_cells(const ens_handle* h);           /* total box cells of all instances    */
+long long ens_active_cells(const ens_handle* h);    /* cells in visited tiles, all instances */
+long long ens_written_cells(const ens_handle* h);
+void* ens_stream(ens_handle* h);
+long long ens_launch_count(const ens_handle* h);
+int ens_destroy(ens_handle* h);
+
+/* ------------------------------------------------------------------------------------
  * Periodic bulk solver (KZM_bulk_ldg_cuda)
  * ------------------------------------------------------------------------------------ */
 typedef struct kzm_params {

@@ -15,7 +15,7 @@ import numpy as np
 from .physics import (bulk_ABC, S_eq, equilibrium_shell_order, estimate_stable_dt_window, DtRequest,
                       boundary_shell_order)
 
-__all__ = ["QSRSolver", "KZMSolver", "load_library", "library_path", "LdgError", "bulk_ABC", "S_eq",
+__all__ = ["QSRSolver", "KZMSolver", "EnsembleSolver", "load_library", "library_path", "LdgError", "bulk_ABC", "S_eq",
            "equilibrium_shell_order", "estimate_stable_dt_window", "DtRequest", "boundary_shell_order"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -70,6 +70,21 @@ class QsrObservables(C.Structure):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
 
 
+class EnsParams(C.Structure):
+    _fields_ = [("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("a", C.c_double), ("b", C.c_double), ("c", C.c_double), ("T_star", C.c_double),
+                ("bulk_modechoice", C.c_int),
+                ("kappa", C.c_double), ("L1", C.c_double), ("L2", C.c_double), ("L3", C.c_double),
+                ("W", C.c_double), ("gamma", C.c_double), ("dt", C.c_double), ("q_norm_cap", C.c_double),
+                ("boundary_custom", C.c_int), ("boundary_S", C.c_double), ("protocol", C.c_int)]
+
+
+class EnsInstance(C.Structure):
+    _fields_ = [("N", C.c_int), ("droplet_radius_cells", C.c_double), ("T_high", C.c_double),
+                ("T_low", C.c_double), ("pre_equil_iters", C.c_longlong), ("ramp_iters", C.c_longlong),
+                ("seed", C.c_ulonglong), ("noise_sigma", C.c_double)]
+
+
 class KzmParams(C.Structure):
     _fields_ = [("Nx", C.c_int), ("Ny", C.c_int), ("Nz", C.c_int),
                 ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
@@ -121,6 +136,19 @@ def load_library():
     L.qsr_observe.argtypes = [C.c_void_p, C.POINTER(QsrObserveArgs), C.POINTER(QsrObservables)]
     L.qsr_sync.argtypes = [C.c_void_p]
     L.qsr_destroy.argtypes = [C.c_void_p]
+    L.ens_create.argtypes = [C.POINTER(EnsParams), C.c_int, C.POINTER(EnsInstance), C.POINTER(C.c_void_p)]
+    L.ens_initial_fields.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+    L.ens_upload.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ens_download.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ens_step.argtypes = [C.c_void_p, C.c_int]
+    L.ens_observe.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrObserveArgs), C.POINTER(QsrObservables)]
+    L.ens_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.ens_destroy.argtypes = [C.c_void_p]
+    for name in ("ens_step_index", "ens_cells", "ens_active_cells", "ens_written_cells", "ens_launch_count"):
+        getattr(L, name).restype = C.c_longlong
+        getattr(L, name).argtypes = [C.c_void_p]
+    L.ens_stream.restype = C.c_void_p
+    L.ens_stream.argtypes = [C.c_void_p]
     L.kzm_create.argtypes = [C.POINTER(KzmParams), C.POINTER(C.c_void_p)]
     L.kzm_upload.argtypes = [C.c_void_p, _dp]
     L.kzm_download.argtypes = [C.c_void_p, _dp]
@@ -240,6 +268,112 @@ class QSRSolver:
     def close(self):
         if getattr(self, "_h", None):
             load_library().qsr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class EnsembleSolver:
+    """Many independent droplets advanced together on one GPU (quench-rate / seed sweeps).
+
+    ``params``: the shared material and solver constants (EnsParams fields: dx dy dz a b c
+    T_star bulk_modechoice kappa L1 L2 L3 W gamma dt q_norm_cap boundary_custom boundary_S
+    protocol). ``instances``: one dict per droplet with keys N droplet_radius_cells T_high
+    T_low pre_equil_iters ramp_iters seed noise_sigma. Each step is one persistent kernel
+    launch over all droplets; the temperature protocol is evaluated on the device.
+    """
+
+    DEFAULTS = dict(dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6, T_star=308.0, bulk_modechoice=1,
+                    kappa=6.5e-12, L1=0.0, L2=0.0, L3=0.0, W=0.0, gamma=0.1, dt=1e-10, q_norm_cap=0.0,
+                    boundary_custom=0, boundary_S=0.5, protocol=2)
+    INSTANCE_DEFAULTS = dict(N=64, droplet_radius_cells=0.0, T_high=315.0, T_low=300.0, pre_equil_iters=0,
+                             ramp_iters=1000, seed=0, noise_sigma=0.0)
+
+    def __init__(self, instances, **params):
+        L = load_library()
+        d = dict(self.DEFAULTS)
+        d.update(params)
+        self.params = d
+        p = EnsParams()
+        for k, v in d.items():
+            setattr(p, k, v)
+        self.instances = []
+        arr = (EnsInstance * len(instances))()
+        for n, inst in enumerate(instances):
+            e = dict(self.INSTANCE_DEFAULTS)
+            e.update(inst)
+            self.instances.append(e)
+            for k, v in e.items():
+                setattr(arr[n], k, v)
+        h = C.c_void_p()
+        _check(L.ens_create(C.byref(p), len(instances), arr, C.byref(h)), "ens_create")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def cells(self, instance) -> int:
+        if not 0 <= instance < len(self.instances):
+            raise LdgError(f"instance {instance} out of range (0..{len(self.instances) - 1})")
+        return int(self.instances[instance]["N"]) ** 3
+
+    def initial_fields(self, init_mode=0, S0=0.5, noise_amplitude=1e-3):
+        _check(load_library().ens_initial_fields(self._h, init_mode, S0, noise_amplitude), "ens_initial_fields")
+
+    def upload(self, instance, q):
+        q = _f64(q)
+        if q.size != 5 * self.cells(instance):
+            raise LdgError(f"upload: expected {5 * self.cells(instance)} doubles, got {q.size}")
+        _check(load_library().ens_upload(self._h, instance, q.ctypes.data_as(_dp)), "ens_upload")
+
+    def download(self, instance) -> np.ndarray:
+        out = np.empty(5 * self.cells(instance))
+        _check(load_library().ens_download(self._h, instance, out.ctypes.data_as(_dp)), "ens_download")
+        return out
+
+    def step(self, n_steps):
+        _check(load_library().ens_step(self._h, int(n_steps)), "ens_step")
+
+    def observe(self, instance, args: QsrObserveArgs | None = None) -> dict:
+        o = QsrObservables()
+        _check(load_library().ens_observe(self._h, instance, C.byref(args) if args is not None else None,
+                                          C.byref(o)), "ens_observe")
+        return o.as_dict()
+
+    def autotune(self, trial_steps=10) -> int:
+        c = C.c_int(0)
+        _check(load_library().ens_autotune(self._h, trial_steps, C.byref(c)), "ens_autotune")
+        return c.value
+
+    @property
+    def step_index(self) -> int:
+        return load_library().ens_step_index(self._h)
+
+    def counts(self) -> dict:
+        L = load_library()
+        return dict(cells=L.ens_cells(self._h), active_cells=L.ens_active_cells(self._h),
+                    written_cells=L.ens_written_cells(self._h))
+
+    def stream(self) -> int:
+        return load_library().ens_stream(self._h)
+
+    def launch_count(self) -> int:
+        return load_library().ens_launch_count(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().ens_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -1051,3 +1051,433 @@ int qsr_destroy(qsr_handle* h) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Ensemble of droplets: every instance is a qsr_handle (geometry, classification, buffers,
+// tensor maps, observables); one persistent work-stealing launch per step covers the active
+// tiles of all instances, and runs of steps are replayed from a captured CUDA graph.
+// ---------------------------------------------------------------------------------------
+struct ens_handle {
+    ens_params p{};
+    std::vector<qsr_handle*> inst;
+    std::vector<ens_instance> desc;
+    std::vector<tiled::EnsInstDev> host_inst;
+    CUtensorMap* d_tms = nullptr;          // 2 per instance: input buffer q[0] / q[1]
+    tiled::EnsInstDev* d_inst = nullptr;
+    tiled::EnsItem* d_items = nullptr;
+    int n_items = 0;
+    tiled::EnsCtl* d_ctl = nullptr;
+    int* d_err = nullptr;
+    int chunk = 0;
+    int grid = 0;
+    size_t smem = 0;
+    bool L2 = false, L3 = false, noise = false;
+    long long step = 0;
+    long long cells = 0, active = 0, written = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+constexpr int kEnsGraphSteps = 32;
+
+using EnsKernel = void (*)(const CUtensorMap*, const tiled::EnsInstDev*, const tiled::EnsItem*, int, tiled::EnsCtl*,
+                           int*);
+
+EnsKernel ens_kernel(bool L2, bool L3, bool N) {
+    using namespace tiled;
+    const int key = (L2 ? 1 : 0) | (L3 ? 2 : 0) | (N ? 4 : 0);
+    switch (key) {
+        case 0: return k_step_ensemble<false, false, false>;
+        case 1: return k_step_ensemble<true, false, false>;
+        case 2: return k_step_ensemble<false, true, false>;
+        case 3: return k_step_ensemble<true, true, false>;
+        case 4: return k_step_ensemble<false, false, true>;
+        case 5: return k_step_ensemble<true, false, true>;
+        case 6: return k_step_ensemble<false, true, true>;
+        default: return k_step_ensemble<true, true, true>;
+    }
+}
+
+void ens_drop_graph(ens_handle* h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_steps = 0;
+}
+
+// Work list of all instances split into chunks of `chunk` planes (instance-major, so CTAs that
+// run together share halo planes of one droplet in L2), and the persistent grid size.
+int ens_rechunk(ens_handle* h, int chunk) {
+    std::vector<tiled::EnsItem> items;
+    for (size_t n = 0; n < h->inst.size(); ++n)
+        for (const int4& t : tiled_items(h->inst[n]->tiled.cols, chunk))
+            items.push_back(tiled::EnsItem{t.x, t.y, t.z, t.w, (int)n, 0, 0, 0});
+    if (h->d_items) cudaFree(h->d_items);
+    h->d_items = nullptr;
+    h->n_items = (int)items.size();
+    if (h->n_items > 0) {
+        int rc = alloc_or_fail((void**)&h->d_items, items.size() * sizeof(tiled::EnsItem));
+        if (rc) return rc;
+        LDG_CUDA(cudaMemcpy(h->d_items, items.data(), items.size() * sizeof(tiled::EnsItem), cudaMemcpyHostToDevice));
+    }
+    h->chunk = chunk;
+    const EnsKernel k = ens_kernel(h->L2, h->L3, h->noise);
+    LDG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    LDG_CUDA(cudaGetDevice(&dev));
+    LDG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    LDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, tiled::THREADS, h->smem));
+    LDG_REQUIRE(per_sm > 0, LDG_ERR_CUDA, "ensemble: step kernel does not fit on an SM");
+    h->grid = std::max(1, std::min(sms * per_sm, h->n_items));
+    ens_drop_graph(h);
+    return LDG_OK;
+}
+
+int ens_launch(ens_handle* h) {
+    const EnsKernel k = ens_kernel(h->L2, h->L3, h->noise);
+    k<<<h->grid, tiled::THREADS, h->smem, h->stream>>>(h->d_tms, h->d_inst, h->d_items, h->n_items, h->d_ctl,
+                                                       h->d_err);
+    LDG_LAUNCHED("k_step_ensemble");
+    return LDG_OK;
+}
+
+// Reads and clears the ensemble's device error word.
+int ens_check(ens_handle* h) {
+    int e = 0;
+    LDG_CUDA(cudaMemcpyAsync(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    if (e != 0) {
+        LDG_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+        LDG_CUDA(cudaStreamSynchronize(h->stream));
+        set_error("ensemble step: a bounded shared-memory pipeline wait gave up");
+        return LDG_ERR_TIMEOUT;
+    }
+    return LDG_OK;
+}
+
+// Makes every instance's current buffer the input of the ensemble's next step.
+void ens_sync_cur(ens_handle* h) {
+    for (qsr_handle* q : h->inst) q->cur = (int)(h->step & 1);
+}
+
+int ens_set_step(ens_handle* h, long long step) {
+    tiled::EnsCtl c{0, 0u, step};
+    LDG_CUDA(cudaMemcpyAsync(h->d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, h->stream));
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    h->step = step;
+    ens_sync_cur(h);
+    return LDG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ens_destroy(ens_handle* h);
+
+int ens_create(const ens_params* params, int n_instances, const ens_instance* instances, ens_handle** out) {
+    clear_error();
+    LDG_REQUIRE(params && instances && out, LDG_ERR_ARG, "ens_create: null argument");
+    LDG_REQUIRE(n_instances >= 1, LDG_ERR_ARG, "ens_create: need at least one instance");
+    const ens_params& p = *params;
+    LDG_REQUIRE(p.dt > 0.0 && std::isfinite(p.dt), LDG_ERR_ARG, "ens_create: dt must be positive and finite");
+    LDG_REQUIRE(p.protocol == 1 || p.protocol == 2, LDG_ERR_ARG, "ens_create: protocol must be 1 (step) or 2 (ramp)");
+    for (int n = 0; n < n_instances; ++n) {
+        LDG_REQUIRE(instances[n].N >= 3, LDG_ERR_ARG, "ens_create: instance grid edge must be >= 3");
+        LDG_REQUIRE(instances[n].pre_equil_iters >= 0 && instances[n].ramp_iters >= 0, LDG_ERR_ARG,
+                    "ens_create: negative protocol length");
+        LDG_REQUIRE(instances[n].noise_sigma >= 0.0, LDG_ERR_ARG, "ens_create: negative noise amplitude");
+    }
+    ens_handle* h = new (std::nothrow) ens_handle();
+    LDG_REQUIRE(h, LDG_ERR_NOMEM, "ens_create: host allocation failed");
+    h->p = p;
+    h->desc.assign(instances, instances + n_instances);
+    h->L2 = p.L2 != 0.0;
+    h->L3 = p.L3 != 0.0;
+    for (int n = 0; n < n_instances; ++n) h->noise = h->noise || instances[n].noise_sigma > 0.0;
+    int rc = LDG_OK;
+    for (int n = 0; n < n_instances && rc == LDG_OK; ++n) {
+        const ens_instance& d = instances[n];
+        qsr_params q{};
+        q.Nx = q.Ny = q.Nz = d.N;
+        q.dx = p.dx; q.dy = p.dy; q.dz = p.dz;
+        q.a = p.a; q.b = p.b; q.c = p.c; q.T_star = p.T_star; q.bulk_modechoice = p.bulk_modechoice;
+        q.kappa = p.kappa; q.L1 = p.L1; q.L2 = p.L2; q.L3 = p.L3; q.W = p.W; q.gamma = p.gamma;
+        q.droplet_radius_cells = d.droplet_radius_cells;
+        qsr_handle* qh = nullptr;
+        rc = qsr_create(&q, &qh);
+        if (rc == LDG_OK) h->inst.push_back(qh);
+    }
+    if (rc != LDG_OK) {
+        const std::string msg = ldg_last_error();
+        ens_destroy(h);
+        set_error(msg);
+        return rc;
+    }
+    // Per-instance descriptors: the static step constants plus the protocol.
+    const double a3 = 3.0 * p.a;
+    const double B = (p.bulk_modechoice == 1) ? (9.0 * p.b) / 2.0 : (27.0 * p.b) / 2.0;
+    const double Cc = (p.bulk_modechoice == 1) ? (9.0 * p.c) / 2.0 : 9.0 * p.c;
+    std::vector<CUtensorMap> tms(2 * (size_t)n_instances);
+    h->host_inst.resize(n_instances);
+    for (int n = 0; n < n_instances; ++n) {
+        qsr_handle* qh = h->inst[n];
+        const ens_instance& d = instances[n];
+        tiled::EnsInstDev& D = h->host_inst[n];
+        D.P = make_const(qh, d.T_high, 0.0, p.dt);
+        D.P.qcap = (float)p.q_norm_cap;
+        D.P.sigma = (float)d.noise_sigma;
+        D.P.key0 = (uint32_t)d.seed;
+        D.P.key1 = (uint32_t)(d.seed >> 32);
+        D.P.instance = 0;
+        D.q[0] = qh->q[0];
+        D.q[1] = qh->q[1];
+        D.flags = qh->flags;
+        D.T_high = d.T_high; D.T_low = d.T_low;
+        D.pre = d.pre_equil_iters; D.ramp = d.ramp_iters;
+        D.protocol = p.protocol;
+        D.custom_shell = p.boundary_custom ? 1 : 0;
+        D.S_custom = p.boundary_S;
+        D.a3 = a3; D.T_star = p.T_star; D.B = B; D.C = Cc;
+        tms[2 * n] = qh->tiled.tmap[0];
+        tms[2 * n + 1] = qh->tiled.tmap[1];
+        h->cells += qh->ncells;
+        h->active += qh->active_cells;
+        h->written += qh->written_cells;
+    }
+    using namespace tiled;
+    h->smem = (h->L2 || h->L3) ? h->inst[0]->tiled.smem_bytes[1] : h->inst[0]->tiled.smem_bytes[0];
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if ((rc = alloc_or_fail((void**)&h->d_tms, tms.size() * sizeof(CUtensorMap))) ||
+        (rc = alloc_or_fail((void**)&h->d_inst, h->host_inst.size() * sizeof(EnsInstDev))) ||
+        (rc = alloc_or_fail((void**)&h->d_ctl, sizeof(EnsCtl))) || (rc = alloc_or_fail((void**)&h->d_err, sizeof(int))) ||
+        e != cudaSuccess) {
+        if (e != cudaSuccess) {
+            set_error(std::string("ens_create: ") + cudaGetErrorString(e));
+            rc = LDG_ERR_CUDA;
+        }
+        ens_destroy(h);
+        return rc;
+    }
+    e = cudaMemcpy(h->d_tms, tms.data(), tms.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h->d_inst, h->host_inst.data(), h->host_inst.size() * sizeof(EnsInstDev), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        set_error(std::string("ens_create: ") + cudaGetErrorString(e));
+        ens_destroy(h);
+        return LDG_ERR_CUDA;
+    }
+    if ((rc = ens_rechunk(h, tiled_default_chunk())) || (rc = ens_set_step(h, 0))) {
+        const std::string msg = ldg_last_error();
+        ens_destroy(h);
+        set_error(msg);
+        return rc;
+    }
+    *out = h;
+    return LDG_OK;
+}
+
+int ens_initial_fields(ens_handle* h, int init_mode, double S0, double noise_amplitude) {
+    clear_error();
+    LDG_REQUIRE(h, LDG_ERR_ARG, "ens_initial_fields: null handle");
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    std::vector<double> buf;
+    for (size_t n = 0; n < h->inst.size(); ++n) {
+        qsr_handle* qh = h->inst[n];
+        buf.resize((size_t)qh->ncells * 5);
+        int rc = qsr_initial_field(qh, init_mode, (long long)h->desc[n].seed, S0, noise_amplitude, buf.data());
+        if (rc == LDG_OK) rc = qsr_upload(qh, buf.data());
+        if (rc) return rc;
+    }
+    ens_sync_cur(h);
+    return LDG_OK;
+}
+
+int ens_upload(ens_handle* h, int instance, const double* q) {
+    clear_error();
+    LDG_REQUIRE(h && q, LDG_ERR_ARG, "ens_upload: null argument");
+    LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_upload: instance out of range");
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    // qsr_upload fills both ping-pong buffers, so either parity of the step index reads it.
+    const int rc = qsr_upload(h->inst[instance], q);
+    ens_sync_cur(h);
+    return rc;
+}
+
+int ens_download(ens_handle* h, int instance, double* q) {
+    clear_error();
+    LDG_REQUIRE(h && q, LDG_ERR_ARG, "ens_download: null argument");
+    LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_download: instance out of range");
+    int rc = ens_check(h);
+    if (rc) return rc;
+    ens_sync_cur(h);
+    return qsr_download(h->inst[instance], q);
+}
+
+int ens_step(ens_handle* h, int n_steps) {
+    clear_error();
+    LDG_REQUIRE(h, LDG_ERR_ARG, "ens_step: null handle");
+    LDG_REQUIRE(n_steps >= 0, LDG_ERR_ARG, "ens_step: n_steps must be >= 0");
+    for (qsr_handle* q : h->inst) LDG_REQUIRE(q->uploaded, LDG_ERR_STATE, "ens_step: an instance has no field");
+    if (h->n_items == 0) {
+        h->step += n_steps;
+        return ens_set_step(h, h->step);
+    }
+    int left = n_steps;
+    while (left >= kEnsGraphSteps) {
+        if (!h->graph) {
+            cudaGraph_t g = nullptr;
+            LDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = LDG_OK;
+            for (int s = 0; s < kEnsGraphSteps && rc == LDG_OK; ++s) rc = ens_launch(h);
+            cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                h->graph = nullptr;
+                set_error(std::string("ens_step: graph capture failed: ") + cudaGetErrorString(e));
+                return LDG_ERR_CUDA;
+            }
+            h->graph_steps = kEnsGraphSteps;
+        }
+        LDG_CUDA(cudaGraphLaunch(h->graph, h->stream));
+        h->launches += h->graph_steps;
+        left -= h->graph_steps;
+    }
+    for (int s = 0; s < left; ++s) {
+        int rc = ens_launch(h);
+        if (rc) return rc;
+        h->launches++;
+    }
+    h->step += n_steps;
+    ens_sync_cur(h);
+    return LDG_OK;
+}
+
+int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_observables* out) {
+    clear_error();
+    LDG_REQUIRE(h && out, LDG_ERR_ARG, "ens_observe: null argument");
+    LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_observe: instance out of range");
+    int rc = ens_check(h);
+    if (rc) return rc;
+    ens_sync_cur(h);
+    qsr_observe_args a{};
+    if (args) {
+        a = *args;
+    } else {
+        const tiled::EnsInstDev& D = h->host_inst[instance];
+        a.T = tiled::ens_temperature(D, h->step);
+        const double A = D.a3 * (a.T - D.T_star);
+        a.S_shell = D.custom_shell ? D.S_custom : std::max(0.0, tiled::ens_S_eq(A, D.B, D.C));
+        const int N = h->desc[instance].N;
+        a.defects_z_slice = N / 2;
+        a.xi_z_slice = N / 2;
+        a.defects_S_threshold = 0.1;
+        a.defects_charge_cutoff = 0.25;
+        a.xi_S_threshold = 0.1;
+        a.want_defects = 1;
+        a.want_xi = 1;
+    }
+    return qsr_observe(h->inst[instance], &a, out);
+}
+
+long long ens_step_index(const ens_handle* h) { return h ? h->step : -1; }
+
+int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk) {
+    clear_error();
+    LDG_REQUIRE(h, LDG_ERR_ARG, "ens_autotune: null handle");
+    LDG_REQUIRE(trial_steps >= 1, LDG_ERR_ARG, "ens_autotune: trial_steps must be >= 1");
+    for (qsr_handle* q : h->inst) LDG_REQUIRE(q->uploaded, LDG_ERR_STATE, "ens_autotune: an instance has no field");
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    // Back up the current field of every instance (the other buffer differs only in cells
+    // the next step rewrites).
+    const long long step0 = h->step;
+    const int w = (int)(step0 & 1);
+    std::vector<float*> backup(h->inst.size(), nullptr);
+    int rc = LDG_OK;
+    for (size_t n = 0; n < h->inst.size() && rc == LDG_OK; ++n) {
+        const size_t bytes = (size_t)h->inst[n]->sc * 5 * sizeof(float);
+        rc = alloc_or_fail((void**)&backup[n], bytes);
+        if (rc == LDG_OK && cudaMemcpyAsync(backup[n], h->inst[n]->q[w], bytes, cudaMemcpyDeviceToDevice, h->stream) !=
+                                cudaSuccess) {
+            set_error("ens_autotune: backup copy failed");
+            rc = LDG_ERR_CUDA;
+        }
+    }
+    const int candidates[] = {8, 12, 16, 24, 32, 48, 64};
+    int best = h->chunk;
+    float best_ms = std::numeric_limits<float>::infinity();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == LDG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) {
+        set_error("ens_autotune: event creation failed");
+        rc = LDG_ERR_CUDA;
+    }
+    for (int c : candidates) {
+        if (rc != LDG_OK) break;
+        if ((rc = ens_rechunk(h, c))) break;
+        for (int s = 0; s < 2 && rc == LDG_OK; ++s) rc = ens_launch(h);
+        if (rc) break;
+        cudaEventRecord(e0, h->stream);
+        for (int s = 0; s < trial_steps && rc == LDG_OK; ++s) rc = ens_launch(h);
+        if (rc) break;
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            set_error("ens_autotune: trial failed");
+            rc = LDG_ERR_CUDA;
+            break;
+        }
+        h->launches += 2 + trial_steps;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = c; }
+        if ((rc = ens_check(h))) break;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    // Restore the fields into both buffers and the step index, whatever happened above.
+    for (size_t n = 0; n < h->inst.size(); ++n) {
+        if (!backup[n]) continue;
+        const size_t bytes = (size_t)h->inst[n]->sc * 5 * sizeof(float);
+        cudaMemcpyAsync(h->inst[n]->q[0], backup[n], bytes, cudaMemcpyDeviceToDevice, h->stream);
+        cudaMemcpyAsync(h->inst[n]->q[1], backup[n], bytes, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    cudaStreamSynchronize(h->stream);
+    for (float* b : backup) cudaFree(b);
+    if (rc != LDG_OK) return rc;
+    if ((rc = ens_rechunk(h, best))) return rc;
+    if ((rc = ens_set_step(h, step0))) return rc;
+    if (chosen_chunk) *chosen_chunk = best;
+    return LDG_OK;
+}
+
+long long ens_cells(const ens_handle* h) { return h ? h->cells : 0; }
+long long ens_active_cells(const ens_handle* h) { return h ? h->active : 0; }
+long long ens_written_cells(const ens_handle* h) { return h ? h->written : 0; }
+void* ens_stream(ens_handle* h) { return h ? (void*)h->stream : nullptr; }
+long long ens_launch_count(const ens_handle* h) {
+    if (!h) return 0;
+    long long n = h->launches;
+    for (const qsr_handle* q : h->inst) n += q->launches;
+    return n;
+}
+
+int ens_destroy(ens_handle* h) {
+    if (!h) return LDG_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    ens_drop_graph(h);
+    for (qsr_handle* q : h->inst) qsr_destroy(q);
+    cudaFree(h->d_tms); cudaFree(h->d_inst); cudaFree(h->d_items); cudaFree(h->d_ctl); cudaFree(h->d_err);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LDG_OK;
+}
+
+}  // extern "C"

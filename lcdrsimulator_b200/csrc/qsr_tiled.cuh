@@ -9,7 +9,8 @@
 // plus a 1-cell halo into a 4-plane shared ring, so each plane costs one CTA barrier. Per cell the kernel then evaluates the chemical potential and
 // the update from shared memory and writes only the cells that change (moving and strongly
 // anchored cells): frozen exterior cells hold identical values in both ping-pong buffers.
-// Tiles that contain no changing cell are never visited (host-built work list).
+// Tiles that contain no changing cell are never visited (host-built work list). The same
+// per-tile routine drives a persistent, work-stealing ensemble kernel over many droplets.
 //
 // mbarrier waits are bounded: on timeout the kernel records LDG_ERR_TIMEOUT in a device
 // word, waits (bounded) for its own TMA loads and returns.
@@ -45,7 +46,7 @@ constexpr int DCSTR = DRW * DROWS;
 constexpr int DPLANE = 3 * DCSTR;
 constexpr int NDS = 4;               // D ring slots: D(i-1) .. D(i+2)
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
-constexpr int CHUNK = 32;            // planes per work item
+constexpr int CHUNK = 16;            // planes per work item (default; tunable)
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -113,66 +114,81 @@ struct SmemD {
     }
 };
 
+// Shared-memory layout of one CTA of the tiled kernels.
+struct TileSmem {
+    float* sq;       // NQ planes of Q (tile + halo, 5 components)
+    float* sd;       // NDS planes of the column divergence
+    uint64_t* bar;   // NQ mbarriers, one per Q slot
+    int* s_abort;    // set when a bounded wait gave up
+    int* s_item;     // work item broadcast (persistent kernel)
+};
+
+template <bool kD>
+__device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
+    TileSmem S;
+    S.sq = reinterpret_cast<float*>(raw);
+    S.sd = S.sq + NQ * PLANE;
+    S.bar = reinterpret_cast<uint64_t*>(S.sd + (kD ? NDS * DPLANE : 0));
+    S.s_abort = reinterpret_cast<int*>(S.bar + NQ);
+    S.s_item = S.s_abort + 1;
+    return S;
+}
+
+// One work item: the (TJ x TK) column tile at (j0, k0) over planes [ib, ie). `phase` holds the
+// parity of the next phase of every slot barrier (bit s for slot s), so a CTA can run many
+// items in a row; every load the item issues is waited for before it returns. Returns false
+// when a bounded wait gave up (the CTA must stop).
 template <bool kL2, bool kL3, bool kNoise, bool kRHS>
-__global__ void __launch_bounds__(THREADS, 1)
-    k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
-                 const int4* __restrict__ items, QsrConst P, int* __restrict__ err) {
+__device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __restrict__ qout,
+                                             const uint8_t* __restrict__ flags, int j0, int k0, int ib, int ie,
+                                             const QsrConst& P, const TileSmem& S, uint32_t& phase,
+                                             int* __restrict__ err) {
     constexpr bool kD = kL2 || kL3;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* sq = reinterpret_cast<float*>(smem_raw);
-    float* sd = sq + NQ * PLANE;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sd + (kD ? NDS * DPLANE : 0));
     // Plane lookahead: with the divergence, step i computes D(i+2), which reads Q(i+3).
     constexpr int LOOK = kD ? 3 : 2;
-    int* s_abort = reinterpret_cast<int*>(bar + NQ);
-
-    const int4 item = items[blockIdx.x];
-    const int j0 = item.x, k0 = item.y, ib = item.z, ie = item.w;
-    const int base = ib - 2;  // first plane this CTA loads; slots and phases count from it
+    float* sq = S.sq;
+    float* sd = S.sd;
+    uint64_t* bar = S.bar;
+    const int base = ib - 2;  // first plane this item loads; slots and phases count from it
     const int tid = threadIdx.x;
     const int kl = tid & (TK - 1), jl = tid / TK;
 
-    // Plane p (p >= base) lives in slot (p - base) % NQ; its load completes that slot's
-    // barrier phase number (p - base) / NQ.
+    // Plane p (p >= base) lives in slot (p - base) % NQ and completes that slot's barrier phase
+    // number (p - base) / NQ of this item.
     auto slot = [&](int p) { return (p - base) % NQ; };
-    auto parity = [&](int p) { return (uint32_t)(((p - base) / NQ) & 1); };
-
-    if (tid == 0) {
-        for (int s = 0; s < NQ; ++s) mbar_init(&bar[s], 1);
-        mbar_fence_init();
-        *s_abort = 0;
-    }
-    __syncthreads();
+    auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (uint32_t)(((p - base) / NQ) & 1); };
 
     // Planes outside the grid complete their phase with a plain arrive (no data).
     auto issue = [&](int p) {
         uint64_t* b = &bar[slot(p)];
         if (p >= 0 && p < P.Nx) {
             mbar_expect_tx(b, PLANE_BYTES);
-            tma_load_4d(sq + slot(p) * PLANE, &tm_in, k0 - HK, j0 - HJ, p, 0, b);
+            tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
             mbar_arrive(b);
         }
     };
-    int issued_end = base + NQ;  // planes [base, issued_end) have been issued (tracked by every thread)
+    int issued_end = base + NQ;  // planes [base, issued_end) issued (same value in every thread)
     if (tid == 0) {
         fence_proxy_async();
         for (int p = base; p < base + NQ; ++p) issue(p);
     }
-    int waited_end = base;       // planes [base, waited_end) have been waited for
+    int waited_end = base;  // planes [base, waited_end) waited for
+    bool ok = true;
     auto wait_plane = [&](int p) {
         if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
             atomicExch(err, LDG_ERR_TIMEOUT);
-            *s_abort = 1;
+            *S.s_abort = 1;
+            ok = false;
         }
         waited_end = p + 1;
     };
 
-    // Column divergence of plane p on the tile plus a 1-cell halo into D slot (p + 4) % 4.
-    // Reads Q planes p-1 .. p+1 (all waited for by the caller).
     // The tile plus its 2-cell halo lies strictly inside the grid in j and k: planes with
     // 2 <= i <= Nx-3 then need no face stencils anywhere (cells, divergence halo, L3).
     const bool tile_interior = (j0 >= 2) && (j0 + TJ + 2 <= P.Ny) && (k0 >= 2) && (k0 + TK + 2 <= P.Nz);
+    // Column divergence of plane p on the tile plus a 1-cell halo into D slot p % NDS.
+    // Reads Q planes p-1 .. p+1 (all waited for by the caller).
     auto compute_D = [&](int p) {
         if (p < 0 || p >= P.Nx) return;
         float* dst = sd + ((p + NDS) % NDS) * DPLANE;
@@ -208,7 +224,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     // Prologue: planes ib-2 .. ib+LOOK-1, then D(ib-1) .. D(ib+1) (visible after the barrier).
     for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     __syncthreads();
-    if (kD && !*s_abort) {
+    if (kD && !*S.s_abort) {
         compute_D(ib - 1);
         compute_D(ib);
         compute_D(ib + 1);
@@ -220,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
     // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
     for (int i = ib; i < ie; ++i) {
-        if (*s_abort) break;  // uniform: read after a barrier
+        if (*S.s_abort) break;  // uniform: read after a barrier
         wait_plane(i + LOOK);
         if (kD) compute_D(i + 2);
         if (in_grid) {
@@ -274,9 +290,150 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         ++issued_end;
     }
-    // Drain: every load this CTA issued lands before its shared memory is released.
+    // Drain: every load this item issued lands before the slots are reused or released.
     for (int p = waited_end; p < issued_end; ++p) {
-        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) atomicExch(err, LDG_ERR_TIMEOUT);
+        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
+            atomicExch(err, LDG_ERR_TIMEOUT);
+            *S.s_abort = 1;
+            ok = false;
+        }
+    }
+    // Advance the per-slot phase parities by the number of loads each slot received.
+    const int n_issued = issued_end - base;
+#pragma unroll
+    for (int s = 0; s < NQ; ++s) {
+        const int uses = (n_issued > s) ? (n_issued - s + NQ - 1) / NQ : 0;
+        phase ^= (uint32_t)(uses & 1) << s;
+    }
+    return ok;
+}
+
+template <bool kD>
+__device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NQ; ++s) mbar_init(&S.bar[s], 1);
+        mbar_fence_init();
+        *S.s_abort = 0;
+    }
+    __syncthreads();
+}
+
+// Single grid: one work item per CTA.
+template <bool kL2, bool kL3, bool kNoise, bool kRHS>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
+                 const int4* __restrict__ items, QsrConst P, int* __restrict__ err) {
+    constexpr bool kD = kL2 || kL3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const TileSmem S = tile_smem<kD>(smem_raw);
+    tile_smem_init<kD>(S);
+    const int4 item = items[blockIdx.x];
+    uint32_t phase = 0;
+    process_tile<kL2, kL3, kNoise, kRHS>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase, err);
+}
+
+// ---------------------------------------------------------------------------------------
+// Ensemble: many independent droplets, one persistent work-stealing launch per step.
+// ---------------------------------------------------------------------------------------
+struct EnsItem {
+    int j0, k0, ib, ie, inst, pad0, pad1, pad2;
+};
+
+// Per-instance descriptor. The step index lives on the device (EnsCtl), so the temperature of
+// the protocol, the shell order and the noise counter are formed in the kernel and one captured
+// CUDA graph can be replayed for any number of steps.
+struct EnsInstDev {
+    QsrConst P;            // static parts (noise key and stream included); cQ, S_shell, step set per step
+    float* q[2];           // ping-pong buffers: input of step s is q[s & 1]
+    const uint8_t* flags;
+    double T_high, T_low;  // protocol (QSR.cu:2679-2687)
+    long long pre, ramp;
+    int protocol;          // 1 step, 2 linear ramp
+    int custom_shell;      // 1: S_shell = S_custom, 0: equilibrium S_eq(T)
+    double S_custom;
+    double a3, T_star, B, C;  // A = a3 (T - T_star); B, C of the bulk convention
+};
+
+struct EnsCtl {
+    int next;            // work-stealing counter (reset by the last CTA of a step)
+    unsigned int done;   // CTAs finished in this step
+    long long step;      // global step index
+};
+
+__host__ __device__ __forceinline__ double ens_temperature(const EnsInstDev& D, long long it) {
+    if (it < D.pre) return D.T_high;
+    if (D.protocol == 1) return D.T_low;
+    const long long t = it - D.pre;
+    if (t <= 0) return D.T_high;
+    if (t >= D.ramp) return D.T_low;
+    return D.T_high + (D.T_low - D.T_high) * ((double)t / (double)D.ramp);
+}
+
+// Lower-energy positive root of 2 C S^2 - B S + 3 A = 0 (QSR.cu:1391-1418), FP64.
+__host__ __device__ __forceinline__ double ens_S_eq(double A, double B, double C) {
+    if (!(C > 0.0)) return 0.0;
+    const double disc = B * B - 24.0 * A * C;
+    if (!(disc > 0.0)) return 0.0;
+    const double sd = sqrt(disc);
+    double best_S = 0.0, best_f = 0.0;
+    const double roots[2] = {(B - sd) / (4.0 * C), (B + sd) / (4.0 * C)};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const double S = roots[r];
+        if (!(S > 0.0)) continue;
+        const double S2 = S * S;
+        const double f = (A / 3.0) * S2 - (2.0 * B / 27.0) * (S2 * S) + (C / 9.0) * (S2 * S2);
+        if (f < best_f) { best_f = f; best_S = S; }
+    }
+    return best_S;
+}
+
+template <bool kL2, bool kL3, bool kNoise>
+__global__ void __launch_bounds__(THREADS, 2)
+    k_step_ensemble(const CUtensorMap* __restrict__ tms, const EnsInstDev* __restrict__ inst,
+                    const EnsItem* __restrict__ items, int n_items, EnsCtl* __restrict__ ctl, int* __restrict__ err) {
+    constexpr bool kD = kL2 || kL3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const TileSmem S = tile_smem<kD>(smem_raw);
+    tile_smem_init<kD>(S);
+    // Every CTA reads the step index before any CTA of this launch finishes (the last CTA to
+    // finish advances it).
+    const long long step = *((volatile long long*)&ctl->step);
+    const int which = (int)(step & 1);
+    uint32_t phase = 0;
+    while (true) {
+        if (threadIdx.x == 0) *S.s_item = atomicAdd(&ctl->next, 1);
+        __syncthreads();
+        const int it = *S.s_item;
+        // Uniform across the CTA: the item and the abort flag are read between two barriers.
+        const bool stop = (it >= n_items) || (*S.s_abort != 0);
+        __syncthreads();
+        if (stop) break;
+        const EnsItem e = items[it];
+        const EnsInstDev& D = inst[e.inst];
+        QsrConst P = D.P;
+        const double T = ens_temperature(D, step);
+        const double A = D.a3 * (T - D.T_star);
+        P.cQ = (float)A;
+        if (!D.custom_shell) {
+            const double s = ens_S_eq(A, D.B, D.C);
+            P.S_shell = (float)(s > 0.0 ? s : 0.0);
+        } else {
+            P.S_shell = (float)D.S_custom;
+        }
+        P.step = step;
+        process_tile<kL2, kL3, kNoise, false>(tms + 2 * e.inst + which, D.q[1 - which], D.flags, e.j0, e.k0, e.ib, e.ie,
+                                              P, S, phase, err);
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int d = atomicAdd(&ctl->done, 1u);
+        if (d == gridDim.x - 1) {
+            ctl->next = 0;
+            ctl->done = 0;
+            ctl->step = step + 1;
+            __threadfence();
+        }
     }
 }
 
@@ -288,11 +445,32 @@ struct TiledPlan {
     long long written_cells = 0;  // cells written per step (moving + strongly anchored)
     int n_items = 0;
     int4* items = nullptr;        // device work list (j0, k0, i_begin, i_end)
+    std::vector<int4> cols;       // host: per active tile column (j0, k0, i_min, i_max + 1)
     int* err = nullptr;           // device error word
     CUtensorMap tmap[2];
     const float* bufs[2] = {nullptr, nullptr};
     size_t smem_bytes[2] = {0, 0};  // [no D, with D]
 };
+
+// Work items of a set of tile columns split into chunks of `chunk` planes, ordered with the
+// plane chunk slowest (CTAs resident together share halo planes in L2).
+inline std::vector<int4> tiled_items(const std::vector<int4>& cols, int chunk) {
+    std::vector<int4> items;
+    for (const int4& c : cols)
+        for (int i = c.z; i < c.w; i += chunk) items.push_back(make_int4(c.x, c.y, i, std::min(c.w, i + chunk)));
+    std::stable_sort(items.begin(), items.end(), [](const int4& a, const int4& b) {
+        if (a.z != b.z) return a.z < b.z;
+        if (a.x != b.x) return a.x < b.x;
+        return a.y < b.y;
+    });
+    return items;
+}
+
+inline int tiled_default_chunk() {
+    int chunk = tiled::CHUNK;
+    if (const char* e = getenv("LDG_QSR_CHUNK")) chunk = std::min(4096, std::max(8, atoi(e)));
+    return chunk;
+}
 
 inline int tiled_encode(CUtensorMap* tm, const float* base, int Nx, int Ny, int Nz, int sj, long long si, long long sc) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -320,16 +498,25 @@ inline int tiled_encode(CUtensorMap* tm, const float* base, int Nx, int Ny, int 
     return LDG_OK;
 }
 
+// Uploads the work list of `plan.cols` split into chunks of `chunk` planes.
+inline int tiled_plan_rechunk(TiledPlan& plan, int chunk) {
+    const std::vector<int4> items = tiled_items(plan.cols, chunk);
+    if (plan.items) cudaFree(plan.items);
+    plan.items = nullptr;
+    plan.n_items = (int)items.size();
+    if (plan.n_items > 0) {
+        LDG_CUDA(cudaMalloc(&plan.items, items.size() * sizeof(int4)));
+        LDG_CUDA(cudaMemcpy(plan.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    return LDG_OK;
+}
+
 // Builds the work list from the host classification and encodes the two tensor maps.
 inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, long long si, const uint8_t* fl,
                             const float* buf0, const float* buf1, long long sc) {
     using namespace tiled;
     plan = TiledPlan{};
     const int ntj = (Ny + TJ - 1) / TJ, ntk = (Nz + TK - 1) / TK;
-    // Planes per work item: CHUNK by default, LDG_QSR_CHUNK (8..4096) to tune.
-    int chunk = CHUNK;
-    if (const char* e = getenv("LDG_QSR_CHUNK")) chunk = std::min(4096, std::max(8, atoi(e)));
-    std::vector<int4> items;
     long long active = 0, written = 0;
     for (int jt = 0; jt < ntj; ++jt)
         for (int kt = 0; kt < ntk; ++kt) {
@@ -337,45 +524,27 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
             for (int i = 0; i < Nx; ++i) {
                 bool any = false;
                 for (int j = jt * TJ; j < std::min(Ny, (jt + 1) * TJ) && !any; ++j)
-                    for (int k = kt * TK; k < std::min(Nz, (kt + 1) * TK); ++k) {
-                        const uint8_t f = fl[(size_t)i * si + (size_t)j * sj + k];
-                        if (f & (kMove | kFixed)) {
-                            any = true;
-                            ++written;
-                        }
-                    }
+                    for (int k = kt * TK; k < std::min(Nz, (kt + 1) * TK); ++k)
+                        if (fl[(size_t)i * si + (size_t)j * sj + k] & (kMove | kFixed)) { any = true; break; }
                 if (any) { imin = std::min(imin, i); imax = std::max(imax, i); }
             }
             if (imax < 0) continue;
             const long long tile_cells = (long long)(std::min(Ny, (jt + 1) * TJ) - jt * TJ) *
                                          (std::min(Nz, (kt + 1) * TK) - kt * TK);
             active += tile_cells * (imax - imin + 1);
-            for (int i = imin; i <= imax; i += chunk)
-                items.push_back(make_int4(jt * TJ, kt * TK, i, std::min(imax + 1, i + chunk)));
+            plan.cols.push_back(make_int4(jt * TJ, kt * TK, imin, imax + 1));
         }
-    // `written` above counts cells per (row) once a row has one; recount exactly.
-    written = 0;
     for (int i = 0; i < Nx; ++i)
         for (int j = 0; j < Ny; ++j)
             for (int k = 0; k < Nz; ++k)
                 if (fl[(size_t)i * si + (size_t)j * sj + k] & (kMove | kFixed)) ++written;
-    // Launch order: plane chunk slowest, so CTAs resident together cover neighbouring tiles of
-    // the same planes and their halo rows are served from L2.
-    std::stable_sort(items.begin(), items.end(), [](const int4& a, const int4& b) {
-        if (a.z != b.z) return a.z < b.z;
-        if (a.x != b.x) return a.x < b.x;
-        return a.y < b.y;
-    });
     plan.active_cells = active;
     plan.written_cells = written;
-    plan.n_items = (int)items.size();
-    if (plan.n_items > 0) {
-        LDG_CUDA(cudaMalloc(&plan.items, items.size() * sizeof(int4)));
-        LDG_CUDA(cudaMemcpy(plan.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    }
+    int rc = tiled_plan_rechunk(plan, tiled_default_chunk());
+    if (rc) return rc;
     LDG_CUDA(cudaMalloc(&plan.err, sizeof(int)));
     LDG_CUDA(cudaMemset(plan.err, 0, sizeof(int)));
-    int rc = tiled_encode(&plan.tmap[0], buf0, Nx, Ny, Nz, sj, si, sc);
+    rc = tiled_encode(&plan.tmap[0], buf0, Nx, Ny, Nz, sj, si, sc);
     if (rc) return rc;
     rc = tiled_encode(&plan.tmap[1], buf1, Nx, Ny, Nz, sj, si, sc);
     if (rc) return rc;
@@ -448,7 +617,7 @@ inline int tiled_check(const TiledPlan& plan, cudaStream_t st) {
 }
 
 inline void tiled_plan_free(TiledPlan& plan) {
-    cudaFree(plan.items);
+    if (plan.items) cudaFree(plan.items);
     cudaFree(plan.err);
     plan = TiledPlan{};
 }
