@@ -54,7 +54,130 @@ WORKLOADS["periodic_quench_512"] = dict(
          "Langevin noise_strength=kT/dx^3 (300 K), init N(0,1e-3) seed 12345",
     N=512, d=1e-8, kappa=6e-12, gamma=0.1, a=0.044e6, b=1.413e6, c=1.153e6, T_star=307.0, T_high=315.0,
     T_low=295.0, ramp=10000, amp=1e-3, seed=12345, log_every=100)
+WORKLOADS["quench_ensemble_128"] = dict(
+    kind="ensemble",
+    desc="128 droplets, R ~ U{16..48} cells (seed 2024) on (2R+8)^3 grids, L1=6e-12 N, strong anchoring with "
+         "equilibrium shell order, linear ramp 315->295 K over tau_Q in {1e3,3e3,1e4,3e4} steps, Langevin "
+         "noise_strength=kT/dx^3 (300 K) with per-droplet Philox seeds, init N(0,1e-3); one persistent launch "
+         "per step over all droplets",
+    n=128, r_lo=16, r_hi=48, seed=2024, taus=(1000, 3000, 10000, 30000), T_high=315.0, T_low=295.0,
+    params=dict(dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6, T_star=307.0, bulk_modechoice=1,
+                kappa=0.0, L1=6e-12, L2=0.0, L3=0.0, W=0.0, gamma=0.1, q_norm_cap=0.0, boundary_custom=0,
+                boundary_S=0.0, protocol=2),
+    amp=1e-3, log_every=100)
 DEFAULT_WORKLOAD = "anisotropic_weak_256"
+
+
+def ensemble_instances(w, rank=0):
+    """The droplet list of the ensemble workload (radii, grids, ramps, seeds)."""
+    rng = np.random.default_rng(w["seed"])
+    radii = rng.integers(w["r_lo"], w["r_hi"] + 1, size=w["n"])
+    out = []
+    for n, R in enumerate(radii):
+        out.append(dict(N=int(2 * R + 8), droplet_radius_cells=float(R), T_high=w["T_high"], T_low=w["T_low"],
+                        pre_equil_iters=0, ramp_iters=int(w["taus"][n % len(w["taus"])]),
+                        seed=int(w["seed"] * 1000 + rank * w["n"] + n), noise_sigma=0.0))
+    return out
+
+
+def ensemble_dt_sigma(w):
+    from lcdrsimulator_b200.physics import DtRequest, estimate_stable_dt_window
+    p = w["params"]
+    r = DtRequest(dx=p["dx"], dy=p["dy"], dz=p["dz"], gamma=p["gamma"], a=p["a"], b=p["b"], c=p["c"],
+                  T_star=p["T_star"], modechoice=p["bulk_modechoice"], kappa=p["kappa"], L1=p["L1"], L2=p["L2"],
+                  L3=p["L3"], S0=0.5, T_a=w["T_high"], T_b=w["T_low"])
+    dt = estimate_stable_dt_window(r)["dt_max"]
+    kT = 1.380649e-23 * 300.0
+    sigma = math.sqrt(2.0 * (1.0 / p["gamma"]) * (kT / p["dx"] ** 3) * dt)
+    return dt, sigma
+
+
+def bench_ensemble(args, w, torch, pg, rank, world, local):
+    """Droplet ensemble (sim_mode 3 quench statistics): one persistent launch per step."""
+    import lcdrsimulator_b200 as L
+    dt, sigma = ensemble_dt_sigma(w)
+    inst = ensemble_instances(w, rank)
+    for d in inst:
+        d["noise_sigma"] = sigma
+    ens = L.EnsembleSolver(inst, dt=dt, **w["params"])
+    ens.initial_fields(init_mode=2, S0=0.5, noise_amplitude=w["amp"])
+    fields = [ens.download(n) for n in range(len(inst))]
+    stream = torch.cuda.ExternalStream(ens.stream())
+    chunk = ens.autotune(trial_steps=10)
+    ens.step(args.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ens.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ens.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    launches = ens.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    c = ens.counts()
+    t_step = ms / 1e3 / args.steps
+    peak, peak_kind = load_peaks()
+    alg = 20 * (c["active_cells"] + c["written_cells"])
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(f).pin_memory().numpy() for f in fields]
+        outs = [torch.empty(f.size, dtype=torch.float64).pin_memory().numpy() for f in fields]
+        ens2 = L.EnsembleSolver(inst, dt=dt, **w["params"])
+        ens2.initial_fields(init_mode=2, S0=0.5, noise_amplitude=w["amp"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for n, f in enumerate(pinned):
+            ens2.upload(n, f)
+        n_obs = 0
+        done = 0
+        while done < args.steps:
+            k = min(w["log_every"], args.steps - done)
+            if done % w["log_every"] == 0:
+                for n in range(len(inst)):
+                    ens2.observe(n)
+                n_obs += 1
+            ens2.step(k)
+            done += k
+        for n, o in enumerate(outs):
+            o[:] = ens2.download(n)
+        t_e2e = time.perf_counter() - t0
+        if pg is not None:
+            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        ens2.close()
+        e2e = {"value": world * c["cells"] * args.steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": 40 * c["cells"] / args.steps,
+               "d2h_bytes_per_step": (40 * c["cells"] + n_obs * len(inst) * 136) / args.steps,
+               "note": "ens_upload of every droplet + K steps + ens_observe of every droplet every 100 steps + "
+                       "ens_download of every droplet; host wall clock around the whole sequence"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": world * c["cells"] * args.steps / (ms / 1e3), "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": args.workload, "desc": w["desc"], "droplets": len(inst),
+                           "box_cells": c["cells"], "active_cells": c["active_cells"],
+                           "written_cells": c["written_cells"], "dt_s": dt, "noise_sigma": sigma,
+                           "chunk": chunk, "parallelism": f"replicas{world}",
+                           "active_cell_updates_per_s": world * c["active_cells"] * args.steps / (ms / 1e3),
+                           "l2": "inputs larger than L2 (two FP32 fields per droplet, %.2f GB)" % (
+                               40 * c["cells"] / 1e9)},
+                "roofline": {"bound": "hbm", "achieved": alg / t_step / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": alg / t_step / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                             "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
+                "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    ens.close()
+    return 0
 
 
 def bench_periodic(args, w, torch, pg, rank, world, local):
@@ -316,6 +439,8 @@ def main():
 
     if w.get("kind") == "periodic":
         return bench_periodic(args, w, torch, pg, rank, world, local)
+    if w.get("kind") == "ensemble":
+        return bench_ensemble(args, w, torch, pg, rank, world, local)
 
     solver = L.QSRSolver(**w["params"])
     geo = solver.geometry()
