@@ -181,6 +181,32 @@ long long ens_launch_count(const ens_handle* h);
 int ens_destroy(ens_handle* h);
 
 /* ------------------------------------------------------------------------------------
+ * Warm-start surrogate: BF16 tcgen05 implicit-GEMM 3x3x3 convolutions (stride 1, zero
+ * padding 1). No counterpart in the reference, which has no learned component; these are the
+ * layers of the 3-D U-Net that predicts a warm-start Q field for the relaxation.
+ * All pointers are DEVICE pointers; work is enqueued on `stream` (NULL = legacy stream).
+ * Activations: NDHWC BF16. Weights: [Co][27][Ci] BF16, tap t = 9(dz+1) + 3(dy+1) + (dx+1).
+ * Ci in {16, 32, 64, 128, 256}; Co a multiple of 16 in [16, 256].
+ * ------------------------------------------------------------------------------------ */
+typedef struct sg_conv_shape {
+    int N, D, H, W, Ci, Co;
+} sg_conv_shape;
+
+/* y = act(conv(x, w) + bias); act 0 = identity, 1 = leaky ReLU (slope 0.01); bias FP32 [Co]
+ * or NULL; y BF16, or FP32 when y_fp32 != 0. */
+int sg_conv3d_fwd(const sg_conv_shape* s, const void* x, const void* w, const float* bias, void* y, int act,
+                  int y_fp32, void* stream);
+/* dw[Co][27][Ci] (FP32, overwritten) = sum over voxels of dy (x) shifted x. */
+int sg_conv3d_wgrad(const sg_conv_shape* s, const void* x, const void* dy, float* dw, void* stream);
+/* wf[Ci][26 - t][Co] = w[Co][t][Ci]: the data gradient of a layer is sg_conv3d_fwd of the
+ * output gradient with wf and the shape's Ci and Co exchanged. */
+int sg_conv3d_flip_weights(const sg_conv_shape* s, const void* w, void* wf, void* stream);
+/* Reads and clears the conv kernels' device error word (LDG_ERR_TIMEOUT when a bounded
+ * pipeline wait gave up); synchronises `stream`. */
+int sg_check(void* stream);
+long long sg_launch_count(void);
+
+/* ------------------------------------------------------------------------------------
  * Periodic bulk solver (KZM_bulk_ldg_cuda)
  * ------------------------------------------------------------------------------------ */
 typedef struct kzm_params {

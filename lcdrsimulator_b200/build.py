@@ -23,7 +23,7 @@ LIB = os.path.join(PKG, "_lib")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp"]
 
-LIB_SOURCES = ["ldg_api_common.cu", "qsr.cu", "kzm.cu"]
+LIB_SOURCES = ["ldg_api_common.cu", "qsr.cu", "kzm.cu", "conv3d_tc.cu"]
 HOST_PROGRAMS = {"qsr_b200": ["qsr_main.cpp"], "kzm_bulk_ldg_b200": ["kzm_main.cpp"]}
 
 
