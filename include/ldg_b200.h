@@ -155,6 +155,8 @@ typedef struct ens_instance {
     long long pre_equil_iters, ramp_iters;
     unsigned long long seed;        /* Philox key of the instance's noise                      */
     double noise_sigma;             /* per-component Langevin amplitude (0 = off)              */
+    int own_material;               /* 1: W, L2, L3 below replace the shared ens_params values */
+    double W, L2, L3;
 } ens_instance;
 
 typedef struct ens_handle ens_handle;
@@ -170,6 +172,7 @@ int ens_step(ens_handle* h, int n_steps);
  * instance's protocol, slices Nz/2, thresholds 0.1 / 0.25. */
 int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_observables* out);
 long long ens_step_index(const ens_handle* h);
+int ens_geometry(const ens_handle* h, int instance, qsr_geometry_info* out);
 /* Times each candidate work-item length (planes per tile item) for trial_steps steps and keeps
  * the fastest; the fields and the step index are restored afterwards. */
 int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk);

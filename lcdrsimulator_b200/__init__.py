@@ -82,7 +82,8 @@ class EnsParams(C.Structure):
 class EnsInstance(C.Structure):
     _fields_ = [("N", C.c_int), ("droplet_radius_cells", C.c_double), ("T_high", C.c_double),
                 ("T_low", C.c_double), ("pre_equil_iters", C.c_longlong), ("ramp_iters", C.c_longlong),
-                ("seed", C.c_ulonglong), ("noise_sigma", C.c_double)]
+                ("seed", C.c_ulonglong), ("noise_sigma", C.c_double), ("own_material", C.c_int),
+                ("W", C.c_double), ("L2", C.c_double), ("L3", C.c_double)]
 
 
 class KzmParams(C.Structure):
@@ -143,6 +144,7 @@ def load_library():
     L.ens_step.argtypes = [C.c_void_p, C.c_int]
     L.ens_observe.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrObserveArgs), C.POINTER(QsrObservables)]
     L.ens_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    L.ens_geometry.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrGeometry)]
     L.ens_destroy.argtypes = [C.c_void_p]
     for name in ("ens_step_index", "ens_cells", "ens_active_cells", "ens_written_cells", "ens_launch_count"):
         getattr(L, name).restype = C.c_longlong
@@ -297,7 +299,7 @@ class EnsembleSolver:
                     kappa=6.5e-12, L1=0.0, L2=0.0, L3=0.0, W=0.0, gamma=0.1, dt=1e-10, q_norm_cap=0.0,
                     boundary_custom=0, boundary_S=0.5, protocol=2)
     INSTANCE_DEFAULTS = dict(N=64, droplet_radius_cells=0.0, T_high=315.0, T_low=300.0, pre_equil_iters=0,
-                             ramp_iters=1000, seed=0, noise_sigma=0.0)
+                             ramp_iters=1000, seed=0, noise_sigma=0.0, own_material=0, W=0.0, L2=0.0, L3=0.0)
 
     def __init__(self, instances, **params):
         L = load_library()
@@ -350,6 +352,11 @@ class EnsembleSolver:
         _check(load_library().ens_observe(self._h, instance, C.byref(args) if args is not None else None,
                                           C.byref(o)), "ens_observe")
         return o.as_dict()
+
+    def geometry(self, instance) -> dict:
+        g = QsrGeometry()
+        _check(load_library().ens_geometry(self._h, instance, C.byref(g)), "ens_geometry")
+        return {f[0]: getattr(g, f[0]) for f in g._fields_}
 
     def autotune(self, trial_steps=10) -> int:
         c = C.c_int(0)

@@ -1197,7 +1197,14 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
     h->desc.assign(instances, instances + n_instances);
     h->L2 = p.L2 != 0.0;
     h->L3 = p.L3 != 0.0;
-    for (int n = 0; n < n_instances; ++n) h->noise = h->noise || instances[n].noise_sigma > 0.0;
+    for (int n = 0; n < n_instances; ++n) {
+        const ens_instance& d = instances[n];
+        h->noise = h->noise || d.noise_sigma > 0.0;
+        if (d.own_material) {
+            h->L2 = h->L2 || d.L2 != 0.0;
+            h->L3 = h->L3 || d.L3 != 0.0;
+        }
+    }
     int rc = LDG_OK;
     for (int n = 0; n < n_instances && rc == LDG_OK; ++n) {
         const ens_instance& d = instances[n];
@@ -1207,6 +1214,9 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
         q.a = p.a; q.b = p.b; q.c = p.c; q.T_star = p.T_star; q.bulk_modechoice = p.bulk_modechoice;
         q.kappa = p.kappa; q.L1 = p.L1; q.L2 = p.L2; q.L3 = p.L3; q.W = p.W; q.gamma = p.gamma;
         q.droplet_radius_cells = d.droplet_radius_cells;
+        if (d.own_material) {
+            q.W = d.W; q.L2 = d.L2; q.L3 = d.L3;
+        }
         qsr_handle* qh = nullptr;
         rc = qsr_create(&q, &qh);
         if (rc == LDG_OK) h->inst.push_back(qh);
@@ -1390,6 +1400,13 @@ int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_o
 }
 
 long long ens_step_index(const ens_handle* h) { return h ? h->step : -1; }
+
+int ens_geometry(const ens_handle* h, int instance, qsr_geometry_info* out) {
+    clear_error();
+    LDG_REQUIRE(h && out, LDG_ERR_ARG, "ens_geometry: null argument");
+    LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_geometry: instance out of range");
+    return qsr_geometry(h->inst[instance], out);
+}
 
 int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk) {
     clear_error();

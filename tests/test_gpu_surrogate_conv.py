@@ -6,9 +6,11 @@ Tolerances (relative to the largest magnitude of the reference):
   * FP32-output forward, data and weight gradient: 1e-4 (FP32 accumulation of exact BF16
     products; only the summation order and the tensor core's internal accumulation differ)
   * BF16-output forward: 1e-2 (one BF16 rounding of the output)
-  * whole U-Net against a reference that rounds activations and their gradients to BF16 at
-    the same points: output 2e-2, per-layer gradient cosine >= 0.9995 and relative L2 <= 3e-2;
-    against the plain FP64 reference: cosine >= 0.98, relative L2 <= 0.25 (BF16 storage)
+  * whole U-Net without activations, against a reference that rounds activations and their
+    gradients to BF16 at the same points: output 1e-2, per-layer gradient cosine >= 0.9999 and
+    relative L2 <= 1.5e-2
+  * whole U-Net with leaky ReLU against the plain FP64 reference: cosine >= 0.98, relative
+    L2 <= 0.25 (activation masks flip where the two forwards straddle zero)
 """
 import numpy as np
 import pytest
@@ -121,30 +123,41 @@ def _cos_l2(a, b):
     return float(torch.nn.functional.cosine_similarity(a, b, dim=0)), float((a - b).norm() / b.norm())
 
 
-def test_unet_matches_cpu_reference_and_gradients():
+def _unet_grads(act: bool, mimic: bool):
     from lcdrsimulator_b200.surrogate import UNet3D
     torch.manual_seed(0)
     net = UNet3D(seed=3).cuda()
+    if not act:
+        for m in net.modules():
+            if hasattr(m, "act"):
+                m.act = 0
     x = bf16_randn(2, 16, 16, 16, 16, scale=0.5)
     r = torch.randn(2, 16, 16, 16, 5)
     out = net(x.cuda())
-    loss = (out[..., :5] * r.cuda()).sum()
-    loss.backward()
-    # BF16-mimicking reference: the same roundings as the GPU path, so only accumulation order
-    # (and the rare rounding flip it causes) differs
-    ref_out, params = unet_ref(net, x, mimic_bf16=True)
+    (out[..., :5] * r.cuda()).sum().backward()
+    ref_out, params = unet_ref(net, x, mimic_bf16=mimic)
     (ref_out[..., :5] * r.double()).sum().backward()
-    assert rel(out.detach(), ref_out.detach()) <= 2e-2
+    return out.detach(), ref_out.detach(), params
+
+
+def test_unet_linear_gradients_match_cpu_reference():
+    # Without activations there are no masks that a slightly different forward value can flip,
+    # so the whole-network gradients must agree with the BF16-rounding reference closely.
+    out, ref, params = _unet_grads(act=False, mimic=True)
+    assert rel(out, ref) <= 1e-2
     for layer, w, b in params:
         cos, l2 = _cos_l2(layer.weight.grad, w.grad)
-        assert cos >= 0.9995 and l2 <= 3e-2, (tuple(w.shape), cos, l2)
+        assert cos >= 0.9999 and l2 <= 1.5e-2, (tuple(w.shape), cos, l2)
         cos, l2 = _cos_l2(layer.bias.grad, b.grad)
-        assert cos >= 0.9995 and l2 <= 3e-2, (tuple(b.shape), cos, l2)
-    # plain FP64 reference: BF16 storage costs a few percent of gradient accuracy, no more
-    ref64, params64 = unet_ref(net, x, mimic_bf16=False)
-    (ref64[..., :5] * r.double()).sum().backward()
-    assert rel(out.detach(), ref64.detach()) <= 2e-2
-    for layer, w, b in params64:
+        assert cos >= 0.9999 and l2 <= 1.5e-2, (tuple(b.shape), cos, l2)
+
+
+def test_unet_gradients_match_cpu_reference():
+    # With leaky ReLU, pre-activations within the forward's BF16 error of zero take the other
+    # slope in one of the two computations; that changes gradients by O(sqrt(fraction flipped)).
+    out, ref, params = _unet_grads(act=True, mimic=False)
+    assert rel(out, ref) <= 2e-2
+    for layer, w, b in params:
         cos, l2 = _cos_l2(layer.weight.grad, w.grad)
         assert cos >= 0.98 and l2 <= 0.25, (tuple(w.shape), cos, l2)
 
@@ -163,6 +176,6 @@ def test_unet_training_reduces_loss():
         loss.backward()
         torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
         opt.step()
-        losses.append(float(loss))
+        losses.append(float(loss.detach()))
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.7 * losses[0], losses
