@@ -96,6 +96,8 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
     """Droplet ensemble (sim_mode 3 quench statistics): one persistent launch per step."""
     import lcdrsimulator_b200 as L
     dt, sigma = ensemble_dt_sigma(w)
+    if args.droplets:
+        w = dict(w, n=args.droplets)
     inst = ensemble_instances(w, rank)
     for d in inst:
         d["noise_sigma"] = sigma
@@ -172,8 +174,8 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
                            "l2": "inputs larger than L2 (two FP32 fields per droplet, %.2f GB)" % (
                                40 * c["cells"] / 1e9)},
                 "roofline": {"bound": "hbm", "achieved": alg / t_step / 1e9, "peak": peak, "unit": "GB/s",
-                             "frac": alg / t_step / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
-                             "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
+                             "frac": alg / t_step / 1e9 / peak, "traffic": load_traffic(args.workload, alg),
+                             "peak_source": peak_kind, "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     ens.close()
@@ -184,7 +186,7 @@ def bench_periodic(args, w, torch, pg, rank, world, local):
     """Periodic bulk quench (the KZM_bulk_ldg path): one kzm_step kernel per step."""
     import lcdrsimulator_b200 as L
     from lcdrsimulator_b200.physics import bulk_ABC, S_eq
-    N, d = w["N"], w["d"]
+    N, d = (args.grid or w["N"]), w["d"]
     # rough explicit limit of the reference (KZM_bulk_ldg.cu:330-349)
     Ah = bulk_ABC(w["a"], w["b"], w["c"], w["T_high"], w["T_star"])[0]
     Al, Bl, Cl = bulk_ABC(w["a"], w["b"], w["c"], w["T_low"], w["T_star"])
@@ -264,8 +266,8 @@ def bench_periodic(args, w, torch, pg, rank, world, local):
                            "noise_sigma": sigma, "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2 (two 5-component FP32 fields of 2.7 GB)"},
                 "roofline": {"bound": "hbm", "achieved": alg / t_step / 1e9, "peak": peak, "unit": "GB/s",
-                             "frac": alg / t_step / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
-                             "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
+                             "frac": alg / t_step / 1e9 / peak, "traffic": load_traffic(args.workload, alg),
+                             "peak_source": peak_kind, "bytes_per_launch": alg, "kernel_ms": t_step * 1e3},
                 "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     s.close()
@@ -287,6 +289,22 @@ def shell_order(w):
         return w["S_shell"]
     p = w["params"]
     return equilibrium_shell_order(p["a"], p["b"], p["c"], w["T"], p["T_star"], p["bulk_modechoice"])
+
+
+def load_traffic(workload, alg_bytes):
+    """DRAM bytes (read + write) per launch of the dominant kernel from the committed ncu
+    summary profiles/traffic.json: measured at full size, or measured on a smaller case and
+    scaled by algorithmic bytes (traffic grows in proportion)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)[workload]
+    except Exception:
+        return None
+    if "bytes_per_launch" in t:
+        return t["bytes_per_launch"]
+    if "traffic_per_algorithmic_byte" in t:
+        return t["traffic_per_algorithmic_byte"] * alg_bytes
+    return None
 
 
 def dist_env():
@@ -421,6 +439,9 @@ def main():
     ap.add_argument("--ref-grid", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--droplets", type=int, default=0,
+                    help="ensemble workload: first N droplets of the distribution (small profiling cases)")
+    ap.add_argument("--grid", type=int, default=0, help="periodic workload: box edge (small profiling cases)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -500,14 +521,7 @@ def main():
     # changing cell's 5 components written once
     alg_bytes = (BYTES_PER_CELL // 2) * (touched + written)
     achieved = alg_bytes / t_step / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "qsr_step_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            tj = json.load(open(tfile))
-            traffic = tj.get("bytes_per_launch_full_size")
-        except Exception:
-            traffic = None
+    traffic = load_traffic(args.workload, alg_bytes)
 
     e2e = None
     if not args.no_e2e:

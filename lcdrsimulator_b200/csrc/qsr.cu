@@ -1144,6 +1144,33 @@ int ens_launch(ens_handle* h) {
     return LDG_OK;
 }
 
+// Captures kEnsGraphSteps launches of the step kernel into a CUDA graph and uploads it, so the
+// first ens_step that replays it pays no instantiation cost. Capturing runs no kernel.
+int ens_build_graph(ens_handle* h) {
+    ens_drop_graph(h);
+    if (h->n_items == 0) return LDG_OK;
+    cudaGraph_t g = nullptr;
+    LDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = LDG_OK;
+    for (int s = 0; s < kEnsGraphSteps && rc == LDG_OK; ++s) rc = ens_launch(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e == cudaSuccess) e = cudaGraphUpload(h->graph, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        ens_drop_graph(h);
+        set_error(std::string("ensemble: graph capture failed: ") + cudaGetErrorString(e));
+        return LDG_ERR_CUDA;
+    }
+    h->graph_steps = kEnsGraphSteps;
+    return LDG_OK;
+}
+
 // Reads and clears the ensemble's device error word.
 int ens_check(ens_handle* h) {
     int e = 0;
@@ -1281,7 +1308,7 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
         ens_destroy(h);
         return LDG_ERR_CUDA;
     }
-    if ((rc = ens_rechunk(h, tiled_default_chunk())) || (rc = ens_set_step(h, 0))) {
+    if ((rc = ens_rechunk(h, tiled_default_chunk())) || (rc = ens_set_step(h, 0)) || (rc = ens_build_graph(h))) {
         const std::string msg = ldg_last_error();
         ens_destroy(h);
         set_error(msg);
@@ -1340,23 +1367,8 @@ int ens_step(ens_handle* h, int n_steps) {
     int left = n_steps;
     while (left >= kEnsGraphSteps) {
         if (!h->graph) {
-            cudaGraph_t g = nullptr;
-            LDG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            int rc = LDG_OK;
-            for (int s = 0; s < kEnsGraphSteps && rc == LDG_OK; ++s) rc = ens_launch(h);
-            cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-            if (rc) {
-                if (g) cudaGraphDestroy(g);
-                return rc;
-            }
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
-            if (g) cudaGraphDestroy(g);
-            if (e != cudaSuccess) {
-                h->graph = nullptr;
-                set_error(std::string("ens_step: graph capture failed: ") + cudaGetErrorString(e));
-                return LDG_ERR_CUDA;
-            }
-            h->graph_steps = kEnsGraphSteps;
+            const int rc = ens_build_graph(h);
+            if (rc) return rc;
         }
         LDG_CUDA(cudaGraphLaunch(h->graph, h->stream));
         h->launches += h->graph_steps;
@@ -1471,6 +1483,7 @@ int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk) {
     if (rc != LDG_OK) return rc;
     if ((rc = ens_rechunk(h, best))) return rc;
     if ((rc = ens_set_step(h, step0))) return rc;
+    if ((rc = ens_build_graph(h))) return rc;
     if (chosen_chunk) *chosen_chunk = best;
     return LDG_OK;
 }
