@@ -233,15 +233,20 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 
     const int j = j0 + jl, k = k0 + kl;
     const bool in_grid = (j < P.Ny) && (k < P.Nz);
+    // The classification of plane i+1 is fetched while plane i is computed (its global-load
+    // latency is then off the critical path).
+    const long long cell0 = (long long)j * P.sj + k;
+    uint8_t f_next = in_grid ? __ldg(flags + (long long)ib * P.si + cell0) : 0;
     // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
     // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
     for (int i = ib; i < ie; ++i) {
         if (*S.s_abort) break;  // uniform: read after a barrier
+        const uint8_t f = f_next;
+        if (in_grid && i + 1 < ie) f_next = __ldg(flags + (long long)(i + 1) * P.si + cell0);
         wait_plane(i + LOOK);
         if (kD) compute_D(i + 2);
         if (in_grid) {
-            const long long id = (long long)i * P.si + (long long)j * P.sj + k;
-            const uint8_t f = __ldg(flags + id);
+            const long long id = (long long)i * P.si + cell0;
             const bool fixed = !kRHS && (f & kFixed);
             const bool move = (f & kMove) != 0;
             if (fixed || move) {

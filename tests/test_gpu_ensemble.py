@@ -27,7 +27,10 @@ CASES = {
         instances=[dict(N=20, T_high=312.0, T_low=300.0, pre_equil_iters=5, ramp_iters=20, seed=11),
                    dict(N=24, T_high=310.0, T_low=302.0, pre_equil_iters=0, ramp_iters=30, seed=12),
                    dict(N=28, droplet_radius_cells=10.0, T_high=309.0, T_low=301.0, pre_equil_iters=12,
-                        ramp_iters=7, seed=13)]),
+                        ramp_iters=7, seed=13),
+                   # large enough for tiles on the face-free interior path
+                   dict(N=72, droplet_radius_cells=30.0, T_high=311.0, T_low=299.0, pre_equil_iters=3,
+                        ramp_iters=25, seed=14)]),
     # strong anchoring, L1 only, step quench, equilibrium shell order S_eq(T)
     "strong_L1_step_equilibrium": dict(
         params=dict(kappa=0.0, L1=6e-12, L2=0.0, L3=0.0, W=0.0, dt=1.5e-10, q_norm_cap=0.0,

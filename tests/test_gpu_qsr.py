@@ -26,6 +26,12 @@ STEP_CASES = {
     "radius_override_weak": dict(Nx=32, Ny=32, Nz=32, droplet_radius_cells=10.0, L1=6e-12, W=1e-5),
     "minimum_grid_3": dict(Nx=3, Ny=3, Nz=3, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5),
     "negative_W": dict(Nx=16, Ny=16, Nz=16, L1=6e-12, W=-1e-6),
+    # grids with tiles whose halo lies inside the grid (k0 = 32, j0 = 8): the face-free interior
+    # path of the tiled kernel, with the droplet surface crossing those tiles
+    "interior_tiles_L1L2L3_weak": dict(Nx=12, Ny=20, Nz=72, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5,
+                                  droplet_radius_cells=9.0),
+    "interior_tiles_L2_strong": dict(Nx=12, Ny=20, Nz=72, L1=6e-12, L2=3e-12, W=0.0, droplet_radius_cells=9.0),
+    "interior_tiles_kappa_weak": dict(Nx=14, Ny=24, Nz=80, L1=0.0, kappa=6.5e-12, W=2e-5, droplet_radius_cells=30.0),
 }
 
 
@@ -129,12 +135,14 @@ def test_long_run_fp32_error_budget(oracle):
     assert eg == pytest.approx(ew, rel=1e-6)
 
 
-def test_noise_stream_matches_philox_box_muller(oracle):
+@pytest.mark.parametrize("grid", [dict(Nx=8, Ny=8, Nz=8), dict(Nx=12, Ny=20, Nz=72, droplet_radius_cells=9.0)])
+def test_noise_stream_matches_philox_box_muller(oracle, grid):
     # With Q = 0, A = 0 (T = T*) and no gradients the update is the noise alone, so the device
     # noise can be read back and compared with Philox4x32-10 + Box-Muller evaluated here.
-    op, solver, d = make_pair(Nx=8, Ny=8, Nz=8, L1=6e-12, W=1e-5)
+    # The second grid has tiles on the face-free interior path.
+    op, solver, d = make_pair(L1=6e-12, W=1e-5, **grid)
     g, fl = oracle.geometry(op)
-    solver.upload(np.zeros(5 * 512))
+    solver.upload(np.zeros(5 * grid["Nx"] * grid["Ny"] * grid["Nz"]))
     sigma, seed, step = 1e-3, 0x1234ABCD5678EF01, 17
     solver.step(1, d["T_star"], 0.0, 1e-12, noise_sigma=sigma, seed=seed, step_index=step)
     got = solver.download().reshape(-1, 5)
