@@ -149,7 +149,7 @@ typedef struct ens_params {
 } ens_params;
 
 typedef struct ens_instance {
-    int N;                          /* cubic grid edge (cells)                                 */
+    int N;                          /* grid extent along x (and y, z unless set below)         */
     double droplet_radius_cells;
     double T_high, T_low;
     long long pre_equil_iters, ramp_iters;
@@ -157,6 +157,7 @@ typedef struct ens_instance {
     double noise_sigma;             /* per-component Langevin amplitude (0 = off)              */
     int own_material;               /* 1: W, L2, L3 below replace the shared ens_params values */
     double W, L2, L3;
+    int Ny, Nz;                     /* grid extents along y and z; 0 = N (cubic)               */
 } ens_instance;
 
 typedef struct ens_handle ens_handle;
@@ -166,6 +167,8 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
 int ens_initial_fields(ens_handle* h, int init_mode, double S0, double noise_amplitude);
 int ens_upload(ens_handle* h, int instance, const double* q_aos5);
 int ens_download(ens_handle* h, int instance, double* q_aos5);
+/* (S, nx, ny, nz) per cell of one instance, FP64, reference cell order (as qsr_nematic). */
+int ens_nematic(ens_handle* h, int instance, double* s_n);
 /* Advances every instance by n_steps (replays a captured CUDA graph of n_steps launches). */
 int ens_step(ens_handle* h, int n_steps);
 /* Observables of one instance at the current step; args NULL: T and S_shell from the

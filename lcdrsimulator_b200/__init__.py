@@ -83,7 +83,7 @@ class EnsInstance(C.Structure):
     _fields_ = [("N", C.c_int), ("droplet_radius_cells", C.c_double), ("T_high", C.c_double),
                 ("T_low", C.c_double), ("pre_equil_iters", C.c_longlong), ("ramp_iters", C.c_longlong),
                 ("seed", C.c_ulonglong), ("noise_sigma", C.c_double), ("own_material", C.c_int),
-                ("W", C.c_double), ("L2", C.c_double), ("L3", C.c_double)]
+                ("W", C.c_double), ("L2", C.c_double), ("L3", C.c_double), ("Ny", C.c_int), ("Nz", C.c_int)]
 
 
 class KzmParams(C.Structure):
@@ -145,6 +145,7 @@ def load_library():
     L.ens_observe.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrObserveArgs), C.POINTER(QsrObservables)]
     L.ens_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     L.ens_geometry.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrGeometry)]
+    L.ens_nematic.argtypes = [C.c_void_p, C.c_int, _dp]
     L.ens_destroy.argtypes = [C.c_void_p]
     for name in ("ens_step_index", "ens_cells", "ens_active_cells", "ens_written_cells", "ens_launch_count"):
         getattr(L, name).restype = C.c_longlong
@@ -299,7 +300,8 @@ class EnsembleSolver:
                     kappa=6.5e-12, L1=0.0, L2=0.0, L3=0.0, W=0.0, gamma=0.1, dt=1e-10, q_norm_cap=0.0,
                     boundary_custom=0, boundary_S=0.5, protocol=2)
     INSTANCE_DEFAULTS = dict(N=64, droplet_radius_cells=0.0, T_high=315.0, T_low=300.0, pre_equil_iters=0,
-                             ramp_iters=1000, seed=0, noise_sigma=0.0, own_material=0, W=0.0, L2=0.0, L3=0.0)
+                             ramp_iters=1000, seed=0, noise_sigma=0.0, own_material=0, W=0.0, L2=0.0, L3=0.0,
+                             Ny=0, Nz=0)
 
     def __init__(self, instances, **params):
         L = load_library()
@@ -328,7 +330,9 @@ class EnsembleSolver:
     def cells(self, instance) -> int:
         if not 0 <= instance < len(self.instances):
             raise LdgError(f"instance {instance} out of range (0..{len(self.instances) - 1})")
-        return int(self.instances[instance]["N"]) ** 3
+        d = self.instances[instance]
+        N = int(d["N"])
+        return N * (int(d["Ny"]) or N) * (int(d["Nz"]) or N)
 
     def initial_fields(self, init_mode=0, S0=0.5, noise_amplitude=1e-3):
         _check(load_library().ens_initial_fields(self._h, init_mode, S0, noise_amplitude), "ens_initial_fields")
@@ -343,6 +347,11 @@ class EnsembleSolver:
         out = np.empty(5 * self.cells(instance))
         _check(load_library().ens_download(self._h, instance, out.ctypes.data_as(_dp)), "ens_download")
         return out
+
+    def nematic(self, instance) -> np.ndarray:
+        out = np.empty(4 * self.cells(instance))
+        _check(load_library().ens_nematic(self._h, instance, out.ctypes.data_as(_dp)), "ens_nematic")
+        return out.reshape(-1, 4)
 
     def step(self, n_steps):
         _check(load_library().ens_step(self._h, int(n_steps)), "ens_step")

@@ -1213,7 +1213,9 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
     LDG_REQUIRE(p.dt > 0.0 && std::isfinite(p.dt), LDG_ERR_ARG, "ens_create: dt must be positive and finite");
     LDG_REQUIRE(p.protocol == 1 || p.protocol == 2, LDG_ERR_ARG, "ens_create: protocol must be 1 (step) or 2 (ramp)");
     for (int n = 0; n < n_instances; ++n) {
-        LDG_REQUIRE(instances[n].N >= 3, LDG_ERR_ARG, "ens_create: instance grid edge must be >= 3");
+        LDG_REQUIRE(instances[n].N >= 3 && (instances[n].Ny == 0 || instances[n].Ny >= 3) &&
+                        (instances[n].Nz == 0 || instances[n].Nz >= 3),
+                    LDG_ERR_ARG, "ens_create: instance grid extents must be >= 3");
         LDG_REQUIRE(instances[n].pre_equil_iters >= 0 && instances[n].ramp_iters >= 0, LDG_ERR_ARG,
                     "ens_create: negative protocol length");
         LDG_REQUIRE(instances[n].noise_sigma >= 0.0, LDG_ERR_ARG, "ens_create: negative noise amplitude");
@@ -1236,7 +1238,9 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
     for (int n = 0; n < n_instances && rc == LDG_OK; ++n) {
         const ens_instance& d = instances[n];
         qsr_params q{};
-        q.Nx = q.Ny = q.Nz = d.N;
+        q.Nx = d.N;
+        q.Ny = d.Ny > 0 ? d.Ny : d.N;
+        q.Nz = d.Nz > 0 ? d.Nz : d.N;
         q.dx = p.dx; q.dy = p.dy; q.dz = p.dz;
         q.a = p.a; q.b = p.b; q.c = p.c; q.T_star = p.T_star; q.bulk_modechoice = p.bulk_modechoice;
         q.kappa = p.kappa; q.L1 = p.L1; q.L2 = p.L2; q.L3 = p.L3; q.W = p.W; q.gamma = p.gamma;
@@ -1355,6 +1359,16 @@ int ens_download(ens_handle* h, int instance, double* q) {
     return qsr_download(h->inst[instance], q);
 }
 
+int ens_nematic(ens_handle* h, int instance, double* s_n) {
+    clear_error();
+    LDG_REQUIRE(h && s_n, LDG_ERR_ARG, "ens_nematic: null argument");
+    LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_nematic: instance out of range");
+    int rc = ens_check(h);
+    if (rc) return rc;
+    ens_sync_cur(h);
+    return qsr_nematic(h->inst[instance], s_n);
+}
+
 int ens_step(ens_handle* h, int n_steps) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "ens_step: null handle");
@@ -1399,9 +1413,9 @@ int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_o
         a.T = tiled::ens_temperature(D, h->step);
         const double A = D.a3 * (a.T - D.T_star);
         a.S_shell = D.custom_shell ? D.S_custom : std::max(0.0, tiled::ens_S_eq(A, D.B, D.C));
-        const int N = h->desc[instance].N;
-        a.defects_z_slice = N / 2;
-        a.xi_z_slice = N / 2;
+        const int Nz = h->inst[instance]->p.Nz;
+        a.defects_z_slice = Nz / 2;
+        a.xi_z_slice = Nz / 2;
         a.defects_S_threshold = 0.1;
         a.defects_charge_cutoff = 0.25;
         a.xi_S_threshold = 0.1;

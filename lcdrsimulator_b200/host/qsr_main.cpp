@@ -11,6 +11,9 @@
 //   noise_seed                 Philox key of the noise (default: random_seed, or 0)
 //   init_file                  warm start from a Qtensor_output_*.dat file (overrides init_mode)
 //   write_iteration_snapshots  single-T per-print nematic dumps (default y, as the reference)
+//   sweep_batched              sim_mode 2: relax every temperature from the same initial field
+//                              at once in one droplet ensemble (default n: the reference's
+//                              sequential continuation)
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -581,6 +584,89 @@ int run_main(int argc, char** argv) {
         const double tau_align = (std::min({rx, ry, rz}) * std::min({rx, ry, rz})) / e.D_total;
         const double min_time = 0.25 * tau_align;
         auto done = [&](double Tv) { return (T_step > 0.0) ? (Tv > T_end + 1e-12) : (Tv < T_end - 1e-12); };
+        if (get<bool>(cfg, "sweep_batched", false)) {
+            // Opt-in batched sweep: every temperature relaxes independently from the same initial
+            // field, all of them at once in one droplet ensemble (one kernel launch per step).
+            // The reference continues each temperature from the previous one's final state, so
+            // results differ from the sequential default; the per-temperature convergence test,
+            // outputs and files are the reference's.
+            std::vector<double> Ts;
+            for (double Tc = T_start; !done(Tc); Tc += T_step) Ts.push_back(Tc);
+            const int nT = (int)Ts.size();
+            ens_params ep{dx, dy, dz, a, b, c, T_star, modechoice, kappa, L1, L2, L3, W, gamma, dt, 0.0,
+                          custom ? 1 : 0, S_custom, 1};
+            std::vector<ens_instance> inst((size_t)nT);
+            for (int n = 0; n < nT; ++n) {
+                ens_instance d{};
+                d.N = Nx; d.Ny = Ny; d.Nz = Nz;
+                d.droplet_radius_cells = radius_cells;
+                d.T_high = Ts[n]; d.T_low = Ts[n];
+                inst[n] = d;
+            }
+            ens_handle* eh = nullptr;
+            check(ens_create(&ep, nT, inst.data(), &eh), "ens_create");
+            for (int n = 0; n < nT; ++n) check(ens_upload(eh, n, h_Q.data()), "ens_upload");
+            std::cout << "\n--- Batched sweep: " << nT << " temperatures from " << T_start << " K to " << Ts.back()
+                      << " K in one ensemble ---" << std::endl;
+            std::vector<char> conv((size_t)nT, 0);
+            std::vector<double> prev_F((size_t)nT, std::numeric_limits<double>::max());
+            std::vector<std::vector<double>> fq((size_t)nT), fn((size_t)nT);
+            std::vector<qsr_observables> fo((size_t)nT);
+            auto obs_args = [&](int n) {
+                return qsr_observe_args{Ts[n], S_shell_at(Ts[n]), defects_slice_default, 0.1, 0.25,
+                                        defects_slice_default, 0.1, 0, 0};
+            };
+            auto capture = [&](int n) {
+                const qsr_observe_args oa = obs_args(n);
+                check(ens_observe(eh, n, &oa, &fo[n]), "ens_observe");
+                fq[n].resize((size_t)(5 * R.n));
+                fn[n].resize((size_t)(4 * R.n));
+                check(ens_download(eh, n, fq[n].data()), "ens_download");
+                check(ens_nematic(eh, n, fn[n].data()), "ens_nematic");
+            };
+            // Checks follow the sequential loop: after steps m * print_freq + 1 (m >= 1).
+            long long steps = 0;
+            int remaining = nT;
+            for (long long next = (long long)printFreq + 1; remaining > 0 && next <= maxIterations;
+                 next += printFreq) {
+                check(ens_step(eh, (int)(next - steps)), "ens_step");
+                steps = next;
+                const double ptime = (double)steps * dt;
+                for (int n = 0; n < nT; ++n) {
+                    if (conv[n]) continue;
+                    const qsr_observe_args oa = obs_args(n);
+                    qsr_observables o{};
+                    check(ens_observe(eh, n, &oa, &o), "ens_observe");
+                    const double F = o.total;
+                    std::cout << "  T = " << Ts[n] << " K, Iter " << (steps - 1) << ", Free Energy: " << F << std::endl;
+                    if (ptime >= min_time && prev_F[n] != 0.0 &&
+                        (std::abs((F - prev_F[n]) / prev_F[n]) < tolerance || F == 0.0)) {
+                        std::cout << "  T = " << Ts[n] << " K: convergence reached at iteration " << (steps - 1)
+                                  << std::endl;
+                        capture(n);
+                        conv[n] = 1;
+                        --remaining;
+                        continue;
+                    }
+                    prev_F[n] = F;
+                }
+            }
+            if (remaining > 0 && steps < maxIterations) check(ens_step(eh, (int)(maxIterations - steps)), "ens_step");
+            for (int n = 0; n < nT; ++n)
+                if (!conv[n]) capture(n);
+            for (int n = 0; n < nT; ++n) {
+                const std::string temp_dir = "output_temp_sweep/T_" + std::to_string(Ts[n]);
+                fs::create_directory(temp_dir);
+                sweep_log << Ts[n] << "," << fo[n].total << "," << fo[n].avg_S << "\n";
+                save_nematic(fn[n], Nx, Ny, Nz, temp_dir + "/nematic_field_final.dat");
+                save_qtensor(fq[n], Nx, Ny, Nz, temp_dir + "/Qtensor_output_final.dat");
+                std::cout << "  Saved final state for T = " << Ts[n] << " K. Average S = " << fo[n].avg_S << std::endl;
+            }
+            sweep_log.flush();
+            ens_destroy(eh);
+            std::cout << "\nSimulation finished." << std::endl;
+            return 0;
+        }
         for (double Tc = T_start; !done(Tc); Tc += T_step) {
             const double S_shell = S_shell_at(Tc);
             std::cout << "\n--- Running simulation for T = " << Tc << " K with S_shell = " << S_shell << " ---\n";

@@ -244,3 +244,45 @@ out_dir = kz
     want = oracle.bulk_step(bp, q0, A, B, C, n=30)
     assert np.abs(got - want).max() <= 2e-6 * np.abs(want).max()
     assert (tmp_path / "kz" / "run_summary.txt").read_text().startswith("Nx=16\nNy=12\nNz=10\n")
+
+
+@pytest.mark.gpu
+def test_qsr_batched_sweep_matches_oracle(tmp_path, oracle):
+    # sweep_batched = y: every temperature relaxes from the same initial field in one ensemble
+    from oracle.oracle import make_params
+    cfg = """sim_mode = 2
+sweep_batched = y
+init_mode = 0
+random_seed = 5
+S0 = 0.5
+Nx = 24
+Ny = 20
+Nz = 28
+T_star = 307
+L1 = 6e-12
+W = 1e-5
+boundary_order_mode = custom
+boundary_S = 0.6
+xi_guard_enabled = n
+iterations = 30
+print_freq = 10
+tolerance = 1e-30
+T_start = 300
+T_end = 302
+T_step = 1
+dt = 1.2e-10
+"""
+    r = run(QSR, cfg, tmp_path)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    rows = (tmp_path / "output_temp_sweep" / "summary.dat").read_text().splitlines()
+    assert rows[0] == "temperature,final_energy_including_anchoring,average_S"
+    assert [float(l.split(",")[0]) for l in rows[1:]] == [300.0, 301.0, 302.0]
+    op = make_params(Nx=24, Ny=20, Nz=28, T_star=307.0, L1=6e-12, W=1e-5)
+    g, fl = oracle.geometry(op)
+    q0 = np.asarray(oracle.init(op, g, 0, 5, 0.5), np.float32).astype(np.float64)
+    for T in (300.0, 301.0, 302.0):
+        d = tmp_path / "output_temp_sweep" / f"T_{T:.6f}"
+        assert (d / "nematic_field_final.dat").exists()
+        q = read_qtensor(d / "Qtensor_output_final.dat", 24 * 20 * 28)
+        want = oracle.step_explicit(op, g, fl, q0, T, 0.6, 1.2e-10, n=30)
+        assert np.abs(q - want).max() <= 1e-5 * np.abs(want).max(), T
