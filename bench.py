@@ -48,6 +48,14 @@ WORKLOADS = {
                     droplet_radius_cells=28.0),
         T=300.0, S_shell=None, S0=0.5, seed=42),
 }
+WORKLOADS["imex_relaxation_256"] = dict(
+    desc="256^3 droplet R=120 cells, L1=6e-12 N, strong anchoring (equilibrium S_shell), T=300 K, random "
+         "directors S0=0.5 seed 42, semi-implicit IMEX step (the reference's sim_mode 3 default): L_stab=L1, "
+         "25 Helmholtz-Jacobi sweeps, dt = 4 dt_max",
+    params=dict(Nx=256, Ny=256, Nz=256, dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6,
+                T_star=307.0, bulk_modechoice=1, kappa=0.0, L1=6e-12, L2=0.0, L3=0.0, W=0.0, gamma=0.1,
+                droplet_radius_cells=120.0),
+    T=300.0, S_shell=None, S0=0.5, seed=42, imex=dict(L_stab=6e-12, jacobi=25, dt_factor=4.0))
 WORKLOADS["periodic_quench_512"] = dict(
     kind="periodic",
     desc="512^3 periodic bulk LdG, kappa=6e-12 N, gamma=0.1, linear ramp 315->295 K over 1e4 steps, "
@@ -485,7 +493,13 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    args_step = solver.step_args(T, S_shell, dt)
+    imex = w.get("imex")
+    if imex:
+        dt = dt * imex["dt_factor"]
+        args_step = solver.step_args(T, S_shell, dt, semi_implicit=True, L_stab=imex["L_stab"],
+                                     jacobi_iters=imex["jacobi"])
+    else:
+        args_step = solver.step_args(T, S_shell, dt)
     for s in range(args.warmup):
         args_step.step_index = s
         solver.step_raw(1, args_step)
@@ -520,6 +534,11 @@ def main():
     # algorithmic bytes per launch: each visited cell's 5 FP32 components read once, each
     # changing cell's 5 components written once
     alg_bytes = (BYTES_PER_CELL // 2) * (touched + written)
+    if imex:
+        # IMEX step: the RHS kernel (visited cells read, moving cells' RHS written) plus the sweep
+        # passes (up to 3 sweeps each), each reading the field and the RHS and writing the field
+        passes = -(-imex["jacobi"] // 3)
+        alg_bytes += passes * 60 * box
     achieved = alg_bytes / t_step / 1e9
     traffic = load_traffic(args.workload, alg_bytes)
 

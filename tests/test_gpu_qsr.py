@@ -72,12 +72,18 @@ def test_q_norm_cap_matches_oracle(oracle):
     assert rel_err(solver.download(), want) <= 2e-6
 
 
-@pytest.mark.parametrize("name", ["L1_strong", "L1L2L3_weak", "odd_grid_all_terms"])
-def test_imex_steps_match_oracle(oracle, name):
-    op, solver, d = make_pair(**STEP_CASES[name])
+IMEX_CASES = dict(STEP_CASES, chunked_planes_strong=dict(Nx=70, Ny=12, Nz=20, L1=6e-12, droplet_radius_cells=9.0))
+
+
+@pytest.mark.parametrize("name,iters", [("L1_strong", 25), ("L1L2L3_weak", 25), ("odd_grid_all_terms", 25),
+                                        ("L1_strong", 2), ("interior_tiles_L2_strong", 7),
+                                        ("chunked_planes_strong", 25), ("chunked_planes_strong", 4)])
+def test_imex_steps_match_oracle(oracle, name, iters):
+    # grids with several 32-plane chunks, interior tiles, odd sweep counts
+    op, solver, d = make_pair(**IMEX_CASES[name])
     g, fl = oracle.geometry(op)
     q0 = fp32(oracle.init(op, g, 0, 7, 0.5))
-    T, S_shell, L_stab, iters = 301.0, 0.6, d["L1"], 25
+    T, S_shell, L_stab = 301.0, 0.6, d["L1"]
     dt = 4 * _dt(d, T)
     solver.upload(q0)
     solver.step(3, T, S_shell, dt, semi_implicit=True, L_stab=L_stab, jacobi_iters=iters)
