@@ -80,17 +80,20 @@ __device__ __forceinline__ void normals5(uint32_t cell, uint32_t instance, long 
     const uint32_t f0 = c[0] & M21, f1 = c[1] & M21, f2 = c[2] & M21, f3 = c[3] & M21;
     const uint32_t f4 = ((c[0] >> 21) << 10) | (c[1] >> 22);  // 11 + 10 bits
     const uint32_t f5 = ((c[2] >> 21) << 10) | (c[3] >> 22);
+    // angle 2 pi u taken as pi + t with t = 2 pi u - pi in (-pi, pi], where the fast hardware
+    // sine/cosine is accurate to ~4e-7: cos(2 pi u) = -cos t, sin(2 pi u) = -sin t
+    constexpr float kTwoPi = 6.28318530717958647692f, kPi = 3.14159265358979323846f;
     float s, co;
     float r = sqrtf(-2.0f * logf(u21(f0)));
-    sincospif(2.0f * u21(f1), &s, &co);
-    g[0] = r * co;
-    g[1] = r * s;
+    __sincosf(fmaf(kTwoPi, u21(f1), -kPi), &s, &co);
+    g[0] = -r * co;
+    g[1] = -r * s;
     r = sqrtf(-2.0f * logf(u21(f2)));
-    sincospif(2.0f * u21(f3), &s, &co);
-    g[2] = r * co;
-    g[3] = r * s;
+    __sincosf(fmaf(kTwoPi, u21(f3), -kPi), &s, &co);
+    g[2] = -r * co;
+    g[3] = -r * s;
     r = sqrtf(-2.0f * logf(u21(f4)));
-    g[4] = r * cospif(2.0f * u21(f5));
+    g[4] = -r * __cosf(fmaf(kTwoPi, u21(f5), -kPi));
 }
 
 // ---------------------------------------------------------------------------------------

@@ -237,6 +237,14 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     // latency is then off the critical path).
     const long long cell0 = (long long)j * P.sj + k;
     uint8_t f_next = in_grid ? __ldg(flags + (long long)ib * P.si + cell0) : 0;
+    // Shared-memory planes of the current step, rolled forward by one plane per step:
+    // Q planes i-2 .. i+2 and divergence planes i-1 .. i+1.
+    const float* qpl[5];
+    const float* dpl[3];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dpl[d] = sd + ((ib + d - 1 + NDS) % NDS) * DPLANE;
     // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
     // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
     for (int i = ib; i < ie; ++i) {
@@ -252,7 +260,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
             if (fixed || move) {
                 SmemQ A;
 #pragma unroll
-                for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(i + d - 2, base)) * PLANE;
+                for (int d = 0; d < 5; ++d) A.pl[d] = qpl[d];
                 A.off = (jl + HJ) * RW + (kl + HK);
                 float c[5], o[5];
 #pragma unroll
@@ -262,7 +270,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                 } else {
                     SmemD DA;
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) DA.pl[d] = sd + ((i + d - 1 + NDS) % NDS) * DPLANE;
+                    for (int d = 0; d < 3; ++d) DA.pl[d] = dpl[d];
                     DA.off = (jl + 1) * DRW + (kl + 1);
                     float mu[5], lap[5];
                     if (tile_interior && i >= 2 && i <= P.Nx - 3)
@@ -294,6 +302,12 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
             issue(issued_end);
         }
         ++issued_end;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
+        qpl[4] = sq + slot(i + 3) * PLANE;
+        dpl[0] = dpl[1];
+        dpl[1] = dpl[2];
+        dpl[2] = sd + ((i + 2 + NDS) % NDS) * DPLANE;
     }
     // Drain: every load this item issued lands before the slots are reused or released.
     for (int p = waited_end; p < issued_end; ++p) {
