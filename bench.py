@@ -121,17 +121,15 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
     time.sleep(0.3)
     l0 = ens.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rank_barrier(pg)
     e0.record(stream)
     ens.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    rank_barrier(pg)
     clocks = sampler.stop()
     launches = ens.launch_count() - l0
-    ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
     c = ens.counts()
     t_step = ms / 1e3 / args.steps
     peak, peak_kind = load_peaks()
@@ -158,11 +156,7 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
             done += k
         for n, o in enumerate(outs):
             o[:] = ens2.download(n)
-        t_e2e = time.perf_counter() - t0
-        if pg is not None:
-            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            t_e2e = float(t.item())
+        t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
         ens2.close()
         e2e = {"value": world * c["cells"] * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": 40 * c["cells"] / args.steps,
@@ -227,17 +221,15 @@ def bench_periodic(args, w, torch, pg, rank, world, local):
     time.sleep(0.3)
     l0 = s.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rank_barrier(pg)
     e0.record(stream)
     for it in range(args.warmup, args.warmup + args.steps):
         step(it)
     e1.record(stream)
     e1.synchronize()
+    rank_barrier(pg)
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(pg, e0.elapsed_time(e1))
     launches = s.launch_count() - l0
     sites = N ** 3
     t_step = ms / 1e3 / args.steps
@@ -260,7 +252,7 @@ def bench_periodic(args, w, torch, pg, rank, world, local):
         s.download(q_out)
         e1.record(stream)
         e1.synchronize()
-        ems = e0.elapsed_time(e1)
+        ems = max_over_ranks(pg, e0.elapsed_time(e1))
         e2e = {"value": world * sites * args.steps / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": (40 * sites + args.steps * 56) / args.steps,
                "d2h_bytes_per_step": (40 * sites + n_obs * 80) / args.steps,
@@ -297,6 +289,26 @@ def shell_order(w):
         return w["S_shell"]
     p = w["params"]
     return equilibrium_shell_order(p["a"], p["b"], p["c"], w["T"], p["T_star"], p["bulk_modechoice"])
+
+
+def max_over_ranks(pg, x, device="cuda"):
+    """Maximum of a per-rank scalar over all ranks (identity without a process group)."""
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_barrier(pg, device="cuda"):
+    """All ranks meet (an all-reduce), then the device is synchronised."""
+    import torch
+    if pg is not None:
+        t = torch.ones(1, device=device)
+        pg.all_reduce(t)
+    if device == "cuda":
+        torch.cuda.synchronize()
 
 
 def load_traffic(workload, alg_bytes):
@@ -481,17 +493,7 @@ def main():
     stream = torch.cuda.ExternalStream(solver.stream())
 
     def barrier():
-        if pg is not None:
-            t = torch.ones(1, device="cuda")
-            pg.all_reduce(t)
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        rank_barrier(pg)
 
     imex = w.get("imex")
     if imex:
@@ -522,7 +524,7 @@ def main():
     barrier()
     clocks = sampler.stop()
     launches = solver.launch_count() - l0
-    ms = max_over_ranks(ms)
+    ms = max_over_ranks(pg, ms)
     box = geo["box_cells"]
     t_step = ms / 1e3 / args.steps
     value = world * box * args.steps / (ms / 1e3)
@@ -564,7 +566,7 @@ def main():
         solver.download(q_out)
         e1.record(stream)
         e1.synchronize()
-        ems = max_over_ranks(e0.elapsed_time(e1))
+        ems = max_over_ranks(pg, e0.elapsed_time(e1))
         barrier()
         field_bytes = 5 * 8 * box
         e2e = {"value": world * box * args.steps / (ems / 1e3), "unit": UNIT,
