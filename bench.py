@@ -459,6 +459,8 @@ def main():
     ap.add_argument("--ref-grid", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--compensated", action="store_true",
+                    help="confined workloads: compensated (hi + lo) field storage")
     ap.add_argument("--droplets", type=int, default=0,
                     help="ensemble workload: first N droplets of the distribution (small profiling cases)")
     ap.add_argument("--grid", type=int, default=0, help="periodic workload: box edge (small profiling cases)")
@@ -483,7 +485,7 @@ def main():
     if w.get("kind") == "ensemble":
         return bench_ensemble(args, w, torch, pg, rank, world, local)
 
-    solver = L.QSRSolver(**w["params"])
+    solver = L.QSRSolver(**dict(w["params"], compensated=1 if args.compensated else 0))
     geo = solver.geometry()
     q0 = solver.initial_field(0, w["seed"], w["S0"])
     dt = dt_max(w)
@@ -536,6 +538,8 @@ def main():
     # algorithmic bytes per launch: each visited cell's 5 FP32 components read once, each
     # changing cell's 5 components written once
     alg_bytes = (BYTES_PER_CELL // 2) * (touched + written)
+    if args.compensated and not imex:
+        alg_bytes += 40 * written  # low words of the changing cells read and written
     if imex:
         # IMEX step: the RHS kernel (visited cells read, moving cells' RHS written) plus the sweep
         # passes (up to 3 sweeps each), each reading the field and the RHS and writing the field
@@ -592,6 +596,7 @@ def main():
                        "box_cells": box, "active_cells": touched, "evolving_cells": geo["evolving_cells"],
                        "active_cell_updates_per_s": world * touched * args.steps / (ms / 1e3),
                        "dt_s": dt, "S_shell": S_shell, "parallelism": f"replicas{world}",
+                       "storage": "compensated hi+lo FP32" if args.compensated else "FP32",
                        "l2": "inputs larger than L2 (two 5-component FP32 fields of 335 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,

@@ -44,6 +44,9 @@ typedef struct qsr_params {
     double W;                       /* anchoring: 0 strong, > 0 Rapini-Papoular (QSR.cu:2113) */
     double gamma;                   /* rotational viscosity (QSR.cu:2114)                     */
     double droplet_radius_cells;    /* <= 0: reference radius 0.5*(min(N)-1) (QSR.cu:151)     */
+    int compensated;                /* 1: compensated storage (hi + lo FP32 words per value) for
+                                       explicit steps: ~48-bit field accumulation, FP32 stencil;
+                                       IMEX steps and the direct kernel reset lo to 0           */
 } qsr_params;
 
 typedef struct qsr_geometry_info {

@@ -35,7 +35,8 @@ class QsrParams(C.Structure):
                 ("a", C.c_double), ("b", C.c_double), ("c", C.c_double), ("T_star", C.c_double),
                 ("bulk_modechoice", C.c_int),
                 ("kappa", C.c_double), ("L1", C.c_double), ("L2", C.c_double), ("L3", C.c_double),
-                ("W", C.c_double), ("gamma", C.c_double), ("droplet_radius_cells", C.c_double)]
+                ("W", C.c_double), ("gamma", C.c_double), ("droplet_radius_cells", C.c_double),
+                ("compensated", C.c_int)]
 
 
 class QsrGeometry(C.Structure):
@@ -176,13 +177,13 @@ class QSRSolver:
     """Confined droplet solver on one GPU (the QSR_cuda hot path).
 
     ``params`` keys: Nx Ny Nz dx dy dz a b c T_star bulk_modechoice kappa L1 L2 L3 W gamma
-    droplet_radius_cells. Fields cross the boundary as host AoS FP64 arrays of shape
+    droplet_radius_cells compensated. Fields cross the boundary as host AoS FP64 arrays of shape
     (Nx*Ny*Nz*5,) in the reference cell order k + Nz*(j + Ny*i).
     """
 
     DEFAULTS = dict(Nx=100, Ny=100, Nz=100, dx=1e-8, dy=1e-8, dz=1e-8, a=0.044e6, b=1.413e6, c=1.153e6,
                     T_star=308.0, bulk_modechoice=1, kappa=6.5e-12, L1=0.0, L2=0.0, L3=0.0, W=0.0, gamma=0.1,
-                    droplet_radius_cells=0.0)
+                    droplet_radius_cells=0.0, compensated=0)
 
     def __init__(self, **params):
         L = load_library()

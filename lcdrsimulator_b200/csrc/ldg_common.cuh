@@ -294,6 +294,44 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
     }
 }
 
+// Explicit update with compensated storage: a cell holds hi + lo (two FP32 words). The
+// increment -(dt/gamma) mu (+ noise) is added to hi exactly (Knuth's TwoSum) and the rounding
+// error carried in lo, so the stored value keeps about 48 significant bits over any number of
+// steps while the stencil arithmetic stays FP32. On return out = new hi, lo = new lo.
+__device__ __forceinline__ void euler_update_comp(const QsrConst& P, const float q[5], float lo[5], const float mu[5],
+                                                  uint32_t cell, bool noise, float out[5]) {
+    float d[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) d[c] = -mu[c] * P.mob_dt;
+    if (noise) {
+        float g[5];
+        normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) d[c] += P.sigma * g[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const float s = __fadd_rn(q[c], d[c]);
+        const float bp = __fsub_rn(s, q[c]);
+        const float e = __fadd_rn(__fsub_rn(q[c], __fsub_rn(s, bp)), __fsub_rn(d[c], bp));
+        const float t = __fadd_rn(e, lo[c]);
+        const float h = __fadd_rn(s, t);
+        lo[c] = __fsub_rn(t, __fsub_rn(h, s));
+        out[c] = h;
+    }
+    if (P.qcap > 0.0f) {
+        const float zz = -out[0] - out[3];
+        const float tr = out[0] * out[0] + out[3] * out[3] + zz * zz +
+                         2.0f * (out[1] * out[1] + out[2] * out[2] + out[4] * out[4]);
+        const float qn = sqrtf(tr > 0.0f ? tr : 0.0f);
+        if (qn > P.qcap && qn > 0.0f) {
+            const float sc = P.qcap / qn;
+#pragma unroll
+            for (int c = 0; c < 5; ++c) { out[c] *= sc; lo[c] *= sc; }
+        }
+    }
+}
+
 // Explicit Euler update with optional Langevin noise and Frobenius cap (QSR.cu:711-731).
 __device__ __forceinline__ void euler_update(const QsrConst& P, const float q[5], const float mu[5], uint32_t cell,
                                              bool noise, float out[5]) {

@@ -168,7 +168,8 @@ __global__ void __launch_bounds__(256) k_jacobi(const float* __restrict__ rhs, c
 
 // Host AoS FP64 (reference cell order) <-> device FP32 SoA.
 __global__ void k_aos_to_soa(const double* __restrict__ aos, float* __restrict__ a, float* __restrict__ b,
-                             int Nx, int Ny, int Nz, int sj, long long si, long long sc) {
+                             int Nx, int Ny, int Nz, int sj, long long si, long long sc, float* __restrict__ la = nullptr,
+                             float* __restrict__ lb = nullptr) {
     const long long n = (long long)Nx * Ny * Nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % Nz);
@@ -178,15 +179,21 @@ __global__ void k_aos_to_soa(const double* __restrict__ aos, float* __restrict__
         const long long id = (long long)i * si + (long long)j * sj + k;
 #pragma unroll
         for (int m = 0; m < 5; ++m) {
-            const float v = (float)aos[5 * t + m];
+            const double x = aos[5 * t + m];
+            const float v = (float)x;
             a[m * sc + id] = v;
             b[m * sc + id] = v;
+            if (la) {
+                const float r = (float)(x - (double)v);  // low word of compensated storage
+                la[m * sc + id] = r;
+                lb[m * sc + id] = r;
+            }
         }
     }
 }
 
 __global__ void k_soa_to_aos(const float* __restrict__ a, double* __restrict__ aos, int Nx, int Ny, int Nz, int sj,
-                             long long si, long long sc) {
+                             long long si, long long sc, const float* __restrict__ lo = nullptr) {
     const long long n = (long long)Nx * Ny * Nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int k = (int)(t % Nz);
@@ -195,7 +202,8 @@ __global__ void k_soa_to_aos(const float* __restrict__ a, double* __restrict__ a
         const int i = (int)(r / Ny);
         const long long id = (long long)i * si + (long long)j * sj + k;
 #pragma unroll
-        for (int m = 0; m < 5; ++m) aos[5 * t + m] = (double)a[m * sc + id];
+        for (int m = 0; m < 5; ++m)
+            aos[5 * t + m] = (double)a[m * sc + id] + (lo ? (double)lo[m * sc + id] : 0.0);
     }
 }
 
@@ -555,6 +563,7 @@ struct qsr_handle {
     int sj = 0;
     long long si = 0, sc = 0, ncells = 0;
     float* q[2] = {nullptr, nullptr};
+    float* lo[2] = {nullptr, nullptr};  // low words of compensated storage (optional)
     float* rhs = nullptr;
     uint8_t* flags = nullptr;
     double* stage = nullptr;       // FP64 AoS staging (5 or 4 doubles per cell)
@@ -721,7 +730,9 @@ int qsr_create(const qsr_params* params, qsr_handle** out) {
         (rc = alloc_or_fail((void**)&h->flags, (size_t)h->sc)) ||
         (rc = alloc_or_fail((void**)&h->opart, (kObsBlocks + 1) * sizeof(ObsPartial))) ||
         (rc = alloc_or_fail((void**)&h->spart, (kSliceBlocks + 1) * sizeof(SlicePartial))) ||
-        (rc = alloc_or_fail((void**)&h->snf, (size_t)2 * p.Nx * p.Ny * 3 * sizeof(double)))) {
+        (rc = alloc_or_fail((void**)&h->snf, (size_t)2 * p.Nx * p.Ny * 3 * sizeof(double))) ||
+        (p.compensated && ((rc = alloc_or_fail((void**)&h->lo[0], fbytes)) ||
+                           (rc = alloc_or_fail((void**)&h->lo[1], fbytes))))) {
         qsr_destroy(h);
         return rc;
     }
@@ -729,6 +740,8 @@ int qsr_create(const qsr_params* params, qsr_handle** out) {
     if (e == cudaSuccess) e = cudaMemcpy(h->flags, fl.data(), (size_t)h->sc, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->q[0], 0, fbytes);
     if (e == cudaSuccess) e = cudaMemset(h->q[1], 0, fbytes);
+    if (e == cudaSuccess && h->lo[0]) e = cudaMemset(h->lo[0], 0, fbytes);
+    if (e == cudaSuccess && h->lo[1]) e = cudaMemset(h->lo[1], 0, fbytes);
     if (e != cudaSuccess) {
         set_error(std::string("qsr_create: ") + cudaGetErrorString(e));
         qsr_destroy(h);
@@ -831,7 +844,8 @@ int qsr_upload(qsr_handle* h, const double* q) {
     LDG_CUDA(cudaMemcpyAsync(h->stage, q, (size_t)h->ncells * 5 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     h->cur = 0;
     k_aos_to_soa<<<grid_blocks(h->ncells, 256, 148 * 16), 256, 0, h->stream>>>(h->stage, h->q[0], h->q[1], h->p.Nx,
-                                                                              h->p.Ny, h->p.Nz, h->sj, h->si, h->sc);
+                                                                              h->p.Ny, h->p.Nz, h->sj, h->si, h->sc,
+                                                                              h->lo[0], h->lo[1]);
     h->launches++;
     LDG_LAUNCHED("k_aos_to_soa");
     LDG_CUDA(cudaStreamSynchronize(h->stream));
@@ -845,7 +859,8 @@ int qsr_download(qsr_handle* h, double* q) {
     int rc = ensure_stage(h, 5);
     if (rc) return rc;
     k_soa_to_aos<<<grid_blocks(h->ncells, 256, 148 * 16), 256, 0, h->stream>>>(h->q[h->cur], h->stage, h->p.Nx,
-                                                                              h->p.Ny, h->p.Nz, h->sj, h->si, h->sc);
+                                                                              h->p.Ny, h->p.Nz, h->sj, h->si, h->sc,
+                                                                              h->lo[h->cur]);
     h->launches++;
     LDG_LAUNCHED("k_soa_to_aos");
     LDG_CUDA(cudaMemcpyAsync(q, h->stage, (size_t)h->ncells * 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -903,7 +918,8 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
         float* outb = h->q[1 - h->cur];
         if (!imex) {
             if (choice == 1 && h->tiled.ok) {
-                int rc = tiled_step(h->tiled, in, outb, h->flags, P, L2, L3, noise, false, h->stream);
+                int rc = tiled_step(h->tiled, in, outb, h->flags, P, L2, L3, noise, false, h->stream, h->lo[h->cur],
+                                    h->lo[1 - h->cur]);
                 if (rc) return rc;
             } else {
                 dispatch_direct<false>(h, in, outb, P, L2, L3, noise);
@@ -932,6 +948,13 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             }
             h->cur = c;
         }
+    }
+    // Compensated storage is kept by the explicit tiled step only; after other updates the
+    // field is its high words.
+    if (h->lo[0] && n_steps > 0 && (imex || choice != 1 || !h->tiled.ok)) {
+        const size_t fbytes = (size_t)h->sc * 5 * sizeof(float);
+        LDG_CUDA(cudaMemsetAsync(h->lo[0], 0, fbytes, h->stream));
+        LDG_CUDA(cudaMemsetAsync(h->lo[1], 0, fbytes, h->stream));
     }
     return LDG_OK;
 }
@@ -1042,7 +1065,7 @@ long long qsr_launch_count(const qsr_handle* h) { return h ? h->launches : 0; }
 int qsr_destroy(qsr_handle* h) {
     if (!h) return LDG_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->rhs); cudaFree(h->flags); cudaFree(h->stage);
+    cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->lo[0]); cudaFree(h->lo[1]); cudaFree(h->rhs); cudaFree(h->flags); cudaFree(h->stage);
     cudaFree(h->opart); cudaFree(h->spart); cudaFree(h->snf);
     tiled_plan_free(h->tiled);
     if (h->stream) cudaStreamDestroy(h->stream);

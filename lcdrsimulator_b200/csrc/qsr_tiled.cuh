@@ -138,11 +138,14 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
 // parity of the next phase of every slot barrier (bit s for slot s), so a CTA can run many
 // items in a row; every load the item issues is waited for before it returns. Returns false
 // when a bounded wait gave up (the CTA must stop).
-template <bool kL2, bool kL3, bool kNoise, bool kRHS>
+// kComp: compensated storage (explicit steps only): the low words of the input cells are read
+// from lo_in and the new low words written to lo_out.
+template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
 __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __restrict__ qout,
                                              const uint8_t* __restrict__ flags, int j0, int k0, int ib, int ie,
                                              const QsrConst& P, const TileSmem& S, uint32_t& phase,
-                                             int* __restrict__ err) {
+                                             int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
+                                             float* __restrict__ lo_out = nullptr) {
     constexpr bool kD = kL2 || kL3;
     // Plane lookahead: with the divergence, step i computes D(i+2), which reads Q(i+3).
     constexpr int LOOK = kD ? 3 : 2;
@@ -267,6 +270,10 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                 for (int m = 0; m < 5; ++m) c[m] = A(m, 0, 0, 0);
                 if (fixed) {
                     surface_q0(P, i, j, k, o);
+                    if (kComp) {
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
+                    }
                 } else {
                     SmemD DA;
 #pragma unroll
@@ -287,6 +294,13 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 #pragma unroll
                             for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
                         }
+                    } else if (kComp) {
+                        float lo[5];
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
+                        euler_update_comp(P, c, lo, mu, cell, kNoise, o);
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
                     } else {
                         euler_update(P, c, mu, cell, kNoise, o);
                     }
@@ -338,17 +352,19 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
 }
 
 // Single grid: one work item per CTA.
-template <bool kL2, bool kL3, bool kNoise, bool kRHS>
+template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
 __global__ void __launch_bounds__(THREADS, 1)
     k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
-                 const int4* __restrict__ items, QsrConst P, int* __restrict__ err) {
+                 const int4* __restrict__ items, QsrConst P, int* __restrict__ err, const float* __restrict__ lo_in,
+                 float* __restrict__ lo_out) {
     constexpr bool kD = kL2 || kL3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const TileSmem S = tile_smem<kD>(smem_raw);
     tile_smem_init<kD>(S);
     const int4 item = items[blockIdx.x];
     uint32_t phase = 0;
-    process_tile<kL2, kL3, kNoise, kRHS>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase, err);
+    process_tile<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase, err,
+                                                lo_in, lo_out);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -575,50 +591,50 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     return LDG_OK;
 }
 
-template <bool L2, bool L3, bool N, bool R>
+template <bool L2, bool L3, bool N, bool R, bool K>
 inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const uint8_t* flags, const QsrConst& P,
-                          cudaStream_t st) {
+                          cudaStream_t st, const float* lo_in, float* lo_out) {
     using namespace tiled;
     constexpr bool kD = L2 || L3;
     const size_t smem = plan.smem_bytes[kD ? 1 : 0];
     static bool configured = false;
     if (!configured) {
-        LDG_CUDA(cudaFuncSetAttribute(k_step_tiled<L2, L3, N, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        LDG_CUDA(cudaFuncSetAttribute(k_step_tiled<L2, L3, N, R, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
         configured = true;
     }
     if (plan.n_items == 0) return LDG_OK;
-    k_step_tiled<L2, L3, N, R><<<plan.n_items, THREADS, smem, st>>>(plan.tmap[which], out, flags, plan.items, P,
-                                                                    plan.err);
+    k_step_tiled<L2, L3, N, R, K><<<plan.n_items, THREADS, smem, st>>>(plan.tmap[which], out, flags, plan.items, P,
+                                                                       plan.err, lo_in, lo_out);
     return LDG_OK;
 }
 
-// One step through the tiled kernel. `in` must be one of the two planned buffers.
-inline int tiled_step(const TiledPlan& plan, const float* in, float* out, const uint8_t* flags, const QsrConst& P,
-                      bool L2, bool L3, bool noise, bool rhs, cudaStream_t st) {
-    const int which = (in == plan.bufs[0]) ? 0 : 1;
+template <bool R, bool K>
+inline int tiled_dispatch(const TiledPlan& plan, int which, float* out, const uint8_t* flags, const QsrConst& P,
+                          bool L2, bool L3, bool noise, cudaStream_t st, const float* lo_in, float* lo_out) {
     const int key = (L2 ? 1 : 0) | (L3 ? 2 : 0) | (noise ? 4 : 0);
-    if (!rhs) {
-        switch (key) {
-            case 0: return tiled_launch_t<false, false, false, false>(plan, which, out, flags, P, st);
-            case 1: return tiled_launch_t<true, false, false, false>(plan, which, out, flags, P, st);
-            case 2: return tiled_launch_t<false, true, false, false>(plan, which, out, flags, P, st);
-            case 3: return tiled_launch_t<true, true, false, false>(plan, which, out, flags, P, st);
-            case 4: return tiled_launch_t<false, false, true, false>(plan, which, out, flags, P, st);
-            case 5: return tiled_launch_t<true, false, true, false>(plan, which, out, flags, P, st);
-            case 6: return tiled_launch_t<false, true, true, false>(plan, which, out, flags, P, st);
-            default: return tiled_launch_t<true, true, true, false>(plan, which, out, flags, P, st);
-        }
-    }
     switch (key) {
-        case 0: return tiled_launch_t<false, false, false, true>(plan, which, out, flags, P, st);
-        case 1: return tiled_launch_t<true, false, false, true>(plan, which, out, flags, P, st);
-        case 2: return tiled_launch_t<false, true, false, true>(plan, which, out, flags, P, st);
-        case 3: return tiled_launch_t<true, true, false, true>(plan, which, out, flags, P, st);
-        case 4: return tiled_launch_t<false, false, true, true>(plan, which, out, flags, P, st);
-        case 5: return tiled_launch_t<true, false, true, true>(plan, which, out, flags, P, st);
-        case 6: return tiled_launch_t<false, true, true, true>(plan, which, out, flags, P, st);
-        default: return tiled_launch_t<true, true, true, true>(plan, which, out, flags, P, st);
+        case 0: return tiled_launch_t<false, false, false, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 1: return tiled_launch_t<true, false, false, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 2: return tiled_launch_t<false, true, false, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 3: return tiled_launch_t<true, true, false, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 4: return tiled_launch_t<false, false, true, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 5: return tiled_launch_t<true, false, true, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        case 6: return tiled_launch_t<false, true, true, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
+        default: return tiled_launch_t<true, true, true, R, K>(plan, which, out, flags, P, st, lo_in, lo_out);
     }
+}
+
+// One step through the tiled kernel. `in` must be one of the two planned buffers. With lo_out
+// set (explicit steps only) the step uses compensated storage: lo_in / lo_out are the low
+// words of the input and output buffers.
+inline int tiled_step(const TiledPlan& plan, const float* in, float* out, const uint8_t* flags, const QsrConst& P,
+                      bool L2, bool L3, bool noise, bool rhs, cudaStream_t st, const float* lo_in = nullptr,
+                      float* lo_out = nullptr) {
+    const int which = (in == plan.bufs[0]) ? 0 : 1;
+    if (rhs) return tiled_dispatch<true, false>(plan, which, out, flags, P, L2, L3, noise, st, nullptr, nullptr);
+    if (lo_out) return tiled_dispatch<false, true>(plan, which, out, flags, P, L2, L3, noise, st, lo_in, lo_out);
+    return tiled_dispatch<false, false>(plan, which, out, flags, P, L2, L3, noise, st, nullptr, nullptr);
 }
 
 // Reads and clears the device error word (LDG_OK when no bounded wait gave up).

@@ -11,6 +11,8 @@
 //   noise_seed                 Philox key of the noise (default: random_seed, or 0)
 //   init_file                  warm start from a Qtensor_output_*.dat file (overrides init_mode)
 //   write_iteration_snapshots  single-T per-print nematic dumps (default y, as the reference)
+//   compensated_storage        keep each field value as two FP32 words (hi + lo) in explicit
+//                              steps: FP64-like accumulation over long runs (default n)
 //   sweep_batched              sim_mode 2: relax every temperature from the same initial field
 //                              at once in one droplet ensemble (default n: the reference's
 //                              sequential continuation)
@@ -330,7 +332,8 @@ int run_main(int argc, char** argv) {
 
     R.Nx = Nx; R.Ny = Ny; R.Nz = Nz;
     R.n = (long long)Nx * Ny * Nz;
-    R.p = qsr_params{Nx, Ny, Nz, dx, dy, dz, a, b, c, T_star, modechoice, kappa, L1, L2, L3, W, gamma, radius_cells};
+    R.p = qsr_params{Nx, Ny, Nz, dx, dy, dz, a, b, c, T_star, modechoice, kappa, L1, L2, L3, W, gamma, radius_cells,
+                     get<bool>(cfg, "compensated_storage", false) ? 1 : 0};
     check(qsr_create(&R.p, &R.h), "qsr_create");
     qsr_geometry_info geo{};
     check(qsr_geometry(R.h, &geo), "qsr_geometry");

@@ -212,3 +212,22 @@ def test_tiled_plan_counts(oracle):
     g, fl = oracle.geometry(op)
     assert geo["written_cells"] == int(((fl & 2) != 0).sum())  # W > 0: moving cells only
     assert geo["written_cells"] <= geo["active_cells"] < geo["box_cells"]
+
+
+def test_compensated_storage_round_trip_and_steps(oracle):
+    # upload / download keep ~48 bits; a few steps stay at the FP32 parity bar
+    op, solver, d = make_pair(Nx=20, Ny=24, Nz=36, L1=6e-12, L2=3e-12, W=1e-5, compensated=1)
+    g, fl = oracle.geometry(op)
+    q0 = np.asarray(oracle.init(op, g, 0, 3, 0.5))
+    solver.upload(q0)
+    assert np.abs(solver.download() - q0).max() <= 1e-13 * np.abs(q0).max()
+    T, S_shell = 302.0, 0.6
+    dt = _dt(d, T)
+    solver.step(5, T, S_shell, dt)
+    want = oracle.step_explicit(op, g, fl, q0, T, S_shell, dt, n=5)
+    assert rel_err(solver.download(), want) <= 2e-6
+    # an IMEX step drops the low words: the field continues from its high words
+    solver.step(1, T, S_shell, dt, semi_implicit=True, L_stab=d["L1"], jacobi_iters=3)
+    q1 = solver.download()
+    solver.upload(q1)
+    assert np.array_equal(np.asarray(q1, np.float32).astype(np.float64), q1)
