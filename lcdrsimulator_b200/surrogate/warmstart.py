@@ -158,9 +158,42 @@ def network_input(q_coarse: np.ndarray, mask: np.ndarray, c: Case) -> np.ndarray
     return x
 
 
+# Cube symmetries: the droplet is a sphere centred in a cubic box and every term of the free
+# energy is rotation invariant, so a relaxed pair (input, target) maps to another valid pair under
+# any of the 48 axis permutations with sign flips R, with Q transformed as Q' = R Q R^T.
+def _q5_to_mat(q):
+    xx, xy, xz, yy, yz = (q[..., i] for i in range(5))
+    zz = -(xx + yy)
+    return torch.stack([torch.stack([xx, xy, xz], -1), torch.stack([xy, yy, yz], -1),
+                        torch.stack([xz, yz, zz], -1)], -2)
+
+
+def _mat_to_q5(m):
+    return torch.stack([m[..., 0, 0], m[..., 0, 1], m[..., 0, 2], m[..., 1, 1], m[..., 1, 2]], -1)
+
+
+def cube_symmetry(x: torch.Tensor, perm, flips, q_slices):
+    """Applies the symmetry (axis permutation `perm`, then sign flips `flips` of the new axes) to
+    a (N, X, Y, Z, C) tensor whose channel slices in `q_slices` hold Q components (5 each)."""
+    y = x.permute(0, 1 + perm[0], 1 + perm[1], 1 + perm[2], 4)
+    dims = [1 + a for a in range(3) if flips[a] < 0]
+    if dims:
+        y = y.flip(dims)
+    R = torch.zeros(3, 3, dtype=torch.float32, device=x.device)
+    for a in range(3):
+        R[a, perm[a]] = float(flips[a])
+    y = y.clone()
+    for sl in q_slices:
+        m = _q5_to_mat(y[..., sl].float())
+        m = torch.einsum("ai,...ij,bj->...ab", R, m, R)
+        y[..., sl] = _mat_to_q5(m).to(y.dtype)
+    return y.contiguous()
+
+
 def train(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, epochs: int = 40, batch: int = 8,
-          lr: float = 1e-3, seed: int = 0, log=None) -> list[float]:
-    """Masked MSE on the 5 scaled Q components; Adam with gradient clipping and cosine decay."""
+          lr: float = 1e-3, seed: int = 0, log=None, augment: bool = True) -> list[float]:
+    """Masked MSE on the 5 scaled Q components; Adam with gradient clipping and cosine decay;
+    each batch transformed by a random cube symmetry when `augment`."""
     dev = torch.device("cuda")
     X = torch.from_numpy(inputs).to(dev, torch.bfloat16)
     Y = torch.from_numpy(targets * Q_SCALE).to(dev, torch.float32)
@@ -176,10 +209,16 @@ def train(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, epoch
         acc = 0.0
         for s in range(0, n, batch):
             idx = perm[s:s + batch].to(dev)
+            xb, yb, m = X[idx], Y[idx], M[idx]
+            if augment:
+                ax = torch.randperm(3, generator=g).tolist()
+                fl = [1 if v else -1 for v in (torch.rand(3, generator=g) < 0.5).tolist()]
+                xb = cube_symmetry(xb, ax, fl, [slice(1, 6)])
+                yb = cube_symmetry(yb, ax, fl, [slice(0, 5)])
+                m = cube_symmetry(m, ax, fl, [])
             opt.zero_grad()
-            out = net(X[idx])[..., :5]
-            m = M[idx]
-            loss = (((out - Y[idx]) ** 2) * m).sum() / (m.sum() * 5)
+            out = net(xb)[..., :5]
+            loss = (((out - yb) ** 2) * m).sum() / (m.sum() * 5)
             loss.backward()
             torch.nn.utils.clip_grad_norm_(net.parameters(), 1.0)
             opt.step()
