@@ -39,6 +39,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--augment", action="store_true", help="random cube-symmetry transform of every batch")
     ap.add_argument("--save", default=None, help="path for the trained weights (torch.save)")
     ap.add_argument("--out", default=None, help="path for the JSON summary")
     args = ap.parse_args(argv)
@@ -58,7 +59,7 @@ def main(argv=None):
     l0 = launch_count()
     t1 = time.time()
     hist = ws.train(net, data["X"], data["Y"], data["M"], epochs=args.epochs, batch=args.batch, lr=args.lr,
-                    seed=args.seed, log=log)
+                    seed=args.seed, log=log, augment=args.augment)
     torch.cuda.synchronize()
     t_train = time.time() - t1
     conv_launches = launch_count() - l0

@@ -191,9 +191,10 @@ def cube_symmetry(x: torch.Tensor, perm, flips, q_slices):
 
 
 def train(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, epochs: int = 40, batch: int = 8,
-          lr: float = 1e-3, seed: int = 0, log=None, augment: bool = True) -> list[float]:
+          lr: float = 1e-3, seed: int = 0, log=None, augment: bool = False) -> list[float]:
     """Masked MSE on the 5 scaled Q components; Adam with gradient clipping and cosine decay;
-    each batch transformed by a random cube symmetry when `augment`."""
+    each batch transformed by a random cube symmetry when `augment` (at 512 training droplets
+    and 80 epochs this under-fits: 2.0x instead of 2.55x time-to-equilibrium speed-up)."""
     dev = torch.device("cuda")
     X = torch.from_numpy(inputs).to(dev, torch.bfloat16)
     Y = torch.from_numpy(targets * Q_SCALE).to(dev, torch.float32)
