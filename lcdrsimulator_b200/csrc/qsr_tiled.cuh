@@ -236,6 +236,8 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 
     const int j = j0 + jl, k = k0 + kl;
     const bool in_grid = (j < P.Ny) && (k < P.Nz);
+    // Cells with 1 <= j <= Ny-2 and 1 <= k <= Nz-2 (and 1 <= i <= Nx-2) need no face stencil.
+    const bool jk_interior = j >= 1 && j <= P.Ny - 2 && k >= 1 && k <= P.Nz - 2;
     // The classification of plane i+1 is fetched while plane i is computed (its global-load
     // latency is then off the critical path).
     const long long cell0 = (long long)j * P.sj + k;
@@ -256,10 +258,14 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         if (in_grid && i + 1 < ie) f_next = __ldg(flags + (long long)(i + 1) * P.si + cell0);
         wait_plane(i + LOOK);
         if (kD) compute_D(i + 2);
+        const bool fixed = in_grid && !kRHS && (f & kFixed);
+        const bool move = in_grid && (f & kMove) != 0;
+        // The face-free form is taken by a whole warp when none of its computing cells touches a
+        // face (exterior cells of a droplet compute nothing, so small droplets use it too).
+        const bool warp_interior =
+            __all_sync(0xffffffffu, !move || (jk_interior && i >= 1 && i <= P.Nx - 2)) != 0;
         if (in_grid) {
             const long long id = (long long)i * P.si + cell0;
-            const bool fixed = !kRHS && (f & kFixed);
-            const bool move = (f & kMove) != 0;
             if (fixed || move) {
                 SmemQ A;
 #pragma unroll
@@ -280,7 +286,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                     for (int d = 0; d < 3; ++d) DA.pl[d] = dpl[d];
                     DA.off = (jl + 1) * DRW + (kl + 1);
                     float mu[5], lap[5];
-                    if (tile_interior && i >= 2 && i <= P.Nx - 3)
+                    if (warp_interior)
                         chem_potential<kL2, kL3, false>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
                     else
                         chem_potential<kL2, kL3, true>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
