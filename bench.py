@@ -504,6 +504,10 @@ def main():
                                      jacobi_iters=imex["jacobi"])
     else:
         args_step = solver.step_args(T, S_shell, dt)
+    # work-item length of the tiled kernel chosen by the library's autotuner (field restored)
+    chunk = solver.autotune(T, S_shell, dt, trial_steps=10,
+                            **({"semi_implicit": True, "L_stab": imex["L_stab"], "jacobi_iters": imex["jacobi"]}
+                               if imex else {}))
     for s in range(args.warmup):
         args_step.step_index = s
         solver.step_raw(1, args_step)
@@ -597,7 +601,7 @@ def main():
                        "box_cells": box, "active_cells": touched, "evolving_cells": geo["evolving_cells"],
                        "active_cell_updates_per_s": world * touched * args.steps / (ms / 1e3),
                        "dt_s": dt, "S_shell": S_shell, "parallelism": f"replicas{world}",
-                       "storage": "compensated hi+lo FP32" if args.compensated else "FP32",
+                       "storage": "compensated hi+lo FP32" if args.compensated else "FP32", "chunk": chunk,
                        "l2": "inputs larger than L2 (two 5-component FP32 fields of 335 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,

@@ -123,6 +123,10 @@ int qsr_observe(qsr_handle* h, const qsr_observe_args* args, qsr_observables* ou
 /* Replaces computeNematicFieldKernel + D2H (QSR.cu:1017-1025, 2816-2821): 4 doubles per
  * cell (S, nx, ny, nz) in the host cell order. */
 int qsr_nematic(qsr_handle* h, double* s_n4);
+/* Tile autotuner: times each candidate work-item length (planes per tile item) for trial_steps
+ * steps with the given step arguments on the uploaded field and keeps the fastest; the field and
+ * the launch count are restored afterwards. No counterpart in the reference (fixed launch shapes). */
+int qsr_autotune(qsr_handle* h, const qsr_step_args* args, int trial_steps, int* chosen_chunk);
 int qsr_sync(qsr_handle* h);
 /* The handle's CUDA stream (a cudaStream_t), for timing with events. */
 void* qsr_stream(qsr_handle* h);

@@ -137,6 +137,7 @@ def load_library():
     L.qsr_step.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrStepArgs)]
     L.qsr_observe.argtypes = [C.c_void_p, C.POINTER(QsrObserveArgs), C.POINTER(QsrObservables)]
     L.qsr_sync.argtypes = [C.c_void_p]
+    L.qsr_autotune.argtypes = [C.c_void_p, C.POINTER(QsrStepArgs), C.c_int, C.POINTER(C.c_int)]
     L.qsr_destroy.argtypes = [C.c_void_p]
     L.ens_create.argtypes = [C.POINTER(EnsParams), C.c_int, C.POINTER(EnsInstance), C.POINTER(C.c_void_p)]
     L.ens_initial_fields.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
@@ -259,6 +260,13 @@ class QSRSolver:
         o = QsrObservables()
         _check(load_library().qsr_observe(self._h, C.byref(a), C.byref(o)), "qsr_observe")
         return o.as_dict()
+
+    def autotune(self, T, S_shell, dt, trial_steps=10, **kw) -> int:
+        """Picks the tiled kernel's work-item length for these step arguments (field restored)."""
+        a = self.step_args(T, S_shell, dt, **kw)
+        c = C.c_int(0)
+        _check(load_library().qsr_autotune(self._h, C.byref(a), int(trial_steps), C.byref(c)), "qsr_autotune")
+        return c.value
 
     def sync(self):
         _check(load_library().qsr_sync(self._h), "qsr_sync")

@@ -1051,6 +1051,66 @@ int qsr_observe(qsr_handle* h, const qsr_observe_args* a, qsr_observables* o) {
     return LDG_OK;
 }
 
+int qsr_autotune(qsr_handle* h, const qsr_step_args* a, int trial_steps, int* chosen_chunk) {
+    clear_error();
+    LDG_REQUIRE(h && a, LDG_ERR_ARG, "qsr_autotune: null argument");
+    LDG_REQUIRE(trial_steps >= 1, LDG_ERR_ARG, "qsr_autotune: trial_steps must be >= 1");
+    LDG_REQUIRE(h->uploaded, LDG_ERR_STATE, "qsr_autotune: no field uploaded");
+    LDG_REQUIRE(h->tiled.ok, LDG_ERR_STATE, "qsr_autotune: no tiled plan");
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    // Back up the current field (and its low words) and the launch count; restore both after.
+    const size_t fbytes = (size_t)h->sc * 5 * sizeof(float);
+    const int planes = h->lo[0] ? 2 : 1;
+    float* backup = nullptr;
+    int rc = alloc_or_fail((void**)&backup, fbytes * planes);
+    if (rc) return rc;
+    const int cur0 = h->cur;
+    const long long launches0 = h->launches;
+    LDG_CUDA(cudaMemcpyAsync(backup, h->q[cur0], fbytes, cudaMemcpyDeviceToDevice, h->stream));
+    if (h->lo[0]) LDG_CUDA(cudaMemcpyAsync(backup + h->sc * 5, h->lo[cur0], fbytes, cudaMemcpyDeviceToDevice, h->stream));
+    const int candidates[] = {8, 12, 16, 24, 32, 48, 64};
+    int best = 0;
+    float best_ms = std::numeric_limits<float>::infinity();
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        set_error("qsr_autotune: event creation failed");
+        rc = LDG_ERR_CUDA;
+    }
+    qsr_step_args t = *a;
+    for (int c : candidates) {
+        if (rc) break;
+        if ((rc = tiled_plan_rechunk(h->tiled, c))) break;
+        if ((rc = qsr_step(h, 2, &t))) break;
+        cudaEventRecord(e0, h->stream);
+        if ((rc = qsr_step(h, trial_steps, &t))) break;
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            set_error("qsr_autotune: trial failed");
+            rc = LDG_ERR_CUDA;
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    // restore both ping-pong buffers from the backup (frozen cells are identical in both)
+    for (int b = 0; b < 2; ++b) {
+        cudaMemcpyAsync(h->q[b], backup, fbytes, cudaMemcpyDeviceToDevice, h->stream);
+        if (h->lo[0]) cudaMemcpyAsync(h->lo[b], backup + h->sc * 5, fbytes, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(backup);
+    h->cur = cur0;
+    h->launches = launches0;
+    if (rc == LDG_OK) rc = tiled_check(h->tiled, h->stream);
+    if (rc) return rc;
+    if ((rc = tiled_plan_rechunk(h->tiled, best))) return rc;
+    if (chosen_chunk) *chosen_chunk = best;
+    return LDG_OK;
+}
+
 int qsr_sync(qsr_handle* h) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "qsr_sync: null handle");

@@ -231,3 +231,20 @@ def test_compensated_storage_round_trip_and_steps(oracle):
     q1 = solver.download()
     solver.upload(q1)
     assert np.array_equal(np.asarray(q1, np.float32).astype(np.float64), q1)
+
+
+def test_autotune_restores_field_and_keeps_results(oracle):
+    op, solver, d = make_pair(**STEP_CASES["interior_tiles_L1L2L3_weak"])
+    g, fl = oracle.geometry(op)
+    q0 = fp32(oracle.init(op, g, 0, 11, 0.5))
+    T, S_shell = 302.0, 0.6
+    dt = _dt(d, T)
+    solver.upload(q0)
+    n0 = solver.launch_count()
+    chunk = solver.autotune(T, S_shell, dt, trial_steps=3)
+    assert chunk in (8, 12, 16, 24, 32, 48, 64)
+    assert solver.launch_count() == n0
+    assert np.array_equal(solver.download(), q0)
+    solver.step(4, T, S_shell, dt)
+    want = oracle.step_explicit(op, g, fl, q0, T, S_shell, dt, n=4)
+    assert rel_err(solver.download(), want) <= 2e-6
