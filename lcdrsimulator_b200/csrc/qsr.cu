@@ -567,6 +567,7 @@ struct qsr_handle {
     float* rhs = nullptr;
     uint8_t* flags = nullptr;
     double* stage = nullptr;       // FP64 AoS staging (5 or 4 doubles per cell)
+    bool stage_shared = false;     // staging owned by an ensemble (shared by its droplets)
     ObsPartial* opart = nullptr;   // kObsBlocks + 1
     SlicePartial* spart = nullptr; // kSliceBlocks + 1
     double* snf = nullptr;         // 2 slices x Nx*Ny x 3
@@ -1125,7 +1126,8 @@ long long qsr_launch_count(const qsr_handle* h) { return h ? h->launches : 0; }
 int qsr_destroy(qsr_handle* h) {
     if (!h) return LDG_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->lo[0]); cudaFree(h->lo[1]); cudaFree(h->rhs); cudaFree(h->flags); cudaFree(h->stage);
+    cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->lo[0]); cudaFree(h->lo[1]); cudaFree(h->rhs); cudaFree(h->flags);
+    if (!h->stage_shared) cudaFree(h->stage);
     cudaFree(h->opart); cudaFree(h->spart); cudaFree(h->snf);
     tiled_plan_free(h->tiled);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1142,6 +1144,7 @@ int qsr_destroy(qsr_handle* h) {
 // ---------------------------------------------------------------------------------------
 struct ens_handle {
     ens_params p{};
+    double* stage = nullptr;               // host-boundary staging shared by all droplets
     std::vector<qsr_handle*> inst;
     std::vector<ens_instance> desc;
     std::vector<tiled::EnsInstDev> host_inst;
@@ -1340,6 +1343,21 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
         ens_destroy(h);
         set_error(msg);
         return rc;
+    }
+    // One FP64 staging buffer for the host boundary of every droplet (calls are sequential and
+    // each synchronises before returning), allocated here rather than on first use.
+    {
+        long long maxc = 0;
+        for (qsr_handle* q : h->inst) maxc = std::max(maxc, q->ncells);
+        rc = alloc_or_fail((void**)&h->stage, (size_t)maxc * 5 * sizeof(double));
+        if (rc) {
+            ens_destroy(h);
+            return rc;
+        }
+        for (qsr_handle* q : h->inst) {
+            q->stage = h->stage;
+            q->stage_shared = true;
+        }
     }
     // Per-instance descriptors: the static step constants plus the protocol.
     const double a3 = 3.0 * p.a;
@@ -1601,6 +1619,7 @@ int ens_destroy(ens_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     ens_drop_graph(h);
     for (qsr_handle* q : h->inst) qsr_destroy(q);
+    cudaFree(h->stage);
     cudaFree(h->d_tms); cudaFree(h->d_inst); cudaFree(h->d_items); cudaFree(h->d_ctl); cudaFree(h->d_err);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
