@@ -353,14 +353,21 @@ __global__ void k_flip_weights(const __nv_bfloat16* __restrict__ w, __nv_bfloat1
 // ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
-int* g_err = nullptr;
+constexpr int kMaxDevices = 64;
+int* g_err_dev[kMaxDevices] = {};  // device error word of each GPU (allocated on first use there)
+int* g_err = nullptr;              // the current device's word (set by ensure_err)
 long long g_launches = 0;
 std::mutex g_mu;
 
 int ensure_err() {
-    if (g_err) return LDG_OK;
-    LDG_CUDA(cudaMalloc(&g_err, sizeof(int)));
-    LDG_CUDA(cudaMemset(g_err, 0, sizeof(int)));
+    int dev = 0;
+    LDG_CUDA(cudaGetDevice(&dev));
+    LDG_REQUIRE(dev >= 0 && dev < kMaxDevices, LDG_ERR_ARG, "conv3d: device index out of range");
+    if (!g_err_dev[dev]) {
+        LDG_CUDA(cudaMalloc(&g_err_dev[dev], sizeof(int)));
+        LDG_CUDA(cudaMemset(g_err_dev[dev], 0, sizeof(int)));
+    }
+    g_err = g_err_dev[dev];
     return LDG_OK;
 }
 
@@ -573,7 +580,8 @@ int sg_conv3d_flip_weights(const sg_conv_shape* s, const void* w, void* wf, void
 int sg_check(void* stream) {
     clear_error();
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_err) return LDG_OK;
+    int rc = ensure_err();
+    if (rc) return rc;
     int e = 0;
     LDG_CUDA(cudaMemcpyAsync(&e, g_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     LDG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));

@@ -608,6 +608,7 @@ struct kzm_handle {
     bool uploaded = false;
     cudaStream_t stream = nullptr;
     long long launches = 0;
+    int device = -1;  // the GPU the handle was created on
 };
 
 extern "C" {
@@ -626,6 +627,7 @@ int kzm_create(const kzm_params* params, kzm_handle** out) {
     kzm_handle* h = new (std::nothrow) kzm_handle();
     LDG_REQUIRE(h, LDG_ERR_NOMEM, "kzm_create: host allocation failed");
     h->p = p;
+    cudaGetDevice(&h->device);
     KzmConst& P = h->base;
     P.Nx = p.Nx; P.Ny = p.Ny; P.Nz = p.Nz;
     P.sy = (p.Nx + 3) & ~3;
@@ -662,6 +664,7 @@ static int kzm_stage(kzm_handle* h) {
 int kzm_upload(kzm_handle* h, const double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "kzm_upload: null argument");
+    DeviceGuard device_guard(h->device);
     int rc = kzm_stage(h);
     if (rc) return rc;
     LDG_CUDA(cudaMemcpyAsync(h->stage, q, (size_t)h->n * 5 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -678,6 +681,7 @@ int kzm_upload(kzm_handle* h, const double* q) {
 int kzm_download(kzm_handle* h, double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "kzm_download: null argument");
+    DeviceGuard device_guard(h->device);
     int rc = kzm_stage(h);
     if (rc) return rc;
     const int blocks = (int)std::min<long long>((h->n + 255) / 256, 148 * 16);
@@ -692,6 +696,7 @@ int kzm_download(kzm_handle* h, double* q) {
 int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
     clear_error();
     LDG_REQUIRE(h && a, LDG_ERR_ARG, "kzm_step: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(n_steps >= 0, LDG_ERR_ARG, "kzm_step: n_steps must be >= 0");
     LDG_REQUIRE(h->uploaded, LDG_ERR_STATE, "kzm_step: no field uploaded");
     LDG_REQUIRE(a->dt > 0.0, LDG_ERR_ARG, "dt must be positive");
@@ -731,6 +736,7 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
 int kzm_observe(kzm_handle* h, double A, double B, double C, kzm_observables* o) {
     clear_error();
     LDG_REQUIRE(h && o, LDG_ERR_ARG, "kzm_observe: null argument");
+    DeviceGuard device_guard(h->device);
     if (!h->nf) {
         int rc = alloc_or_fail((void**)&h->nf, (size_t)h->n * sizeof(double4));
         if (rc) return rc;
@@ -856,6 +862,7 @@ long long kzm_launch_count(const kzm_handle* h) { return h ? h->launches : 0; }
 
 int kzm_destroy(kzm_handle* h) {
     if (!h) return LDG_OK;
+    DeviceGuard device_guard(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->stage); cudaFree(h->nf); cudaFree(h->part);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -41,4 +41,20 @@ void clear_error();
         }                                                                                       \
     } while (0)
 
+// Makes a handle's device current for the scope of an entry point and restores the caller's
+// device afterwards, so handles created on different GPUs can be used from one thread.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        int cur = -1;
+        if (dev < 0 || cudaGetDevice(&cur) != cudaSuccess || cur == dev) return;
+        if (cudaSetDevice(dev) == cudaSuccess) prev = cur;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 }  // namespace ldg

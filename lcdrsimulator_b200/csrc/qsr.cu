@@ -576,6 +576,7 @@ struct qsr_handle {
     bool uploaded = false;
     cudaStream_t stream = nullptr;
     long long launches = 0;
+    int device = -1;               // the GPU the handle was created on
 };
 
 namespace {
@@ -670,6 +671,7 @@ int qsr_create(const qsr_params* params, qsr_handle** out) {
     qsr_handle* h = new (std::nothrow) qsr_handle();
     LDG_REQUIRE(h, LDG_ERR_NOMEM, "qsr_create: host allocation failed");
     h->p = p;
+    cudaGetDevice(&h->device);
     h->g = make_geometry(p);
     h->sj = (p.Nz + 3) & ~3;
     h->si = (long long)p.Ny * h->sj;
@@ -840,6 +842,7 @@ static int ensure_stage(qsr_handle* h, size_t doubles) {
 int qsr_upload(qsr_handle* h, const double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "qsr_upload: null argument");
+    DeviceGuard device_guard(h->device);
     int rc = ensure_stage(h, 5);
     if (rc) return rc;
     LDG_CUDA(cudaMemcpyAsync(h->stage, q, (size_t)h->ncells * 5 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -857,6 +860,7 @@ int qsr_upload(qsr_handle* h, const double* q) {
 int qsr_download(qsr_handle* h, double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "qsr_download: null argument");
+    DeviceGuard device_guard(h->device);
     int rc = ensure_stage(h, 5);
     if (rc) return rc;
     k_soa_to_aos<<<grid_blocks(h->ncells, 256, 148 * 16), 256, 0, h->stream>>>(h->q[h->cur], h->stage, h->p.Nx,
@@ -872,6 +876,7 @@ int qsr_download(qsr_handle* h, double* q) {
 int qsr_nematic(qsr_handle* h, double* s_n) {
     clear_error();
     LDG_REQUIRE(h && s_n, LDG_ERR_ARG, "qsr_nematic: null argument");
+    DeviceGuard device_guard(h->device);
     int rc = ensure_stage(h, 5);
     if (rc) return rc;
     k_nematic_out<<<grid_blocks(h->ncells, 256, 148 * 16), 256, 0, h->stream>>>(h->q[h->cur], h->stage, h->p.Nx,
@@ -886,6 +891,7 @@ int qsr_nematic(qsr_handle* h, double* s_n) {
 int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
     clear_error();
     LDG_REQUIRE(h && a, LDG_ERR_ARG, "qsr_step: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(n_steps >= 0, LDG_ERR_ARG, "qsr_step: n_steps must be >= 0");
     LDG_REQUIRE(h->uploaded, LDG_ERR_STATE, "qsr_step: no field uploaded");
     LDG_REQUIRE(a->dt > 0.0 && std::isfinite(a->dt), LDG_ERR_ARG, "qsr_step: dt must be positive and finite");
@@ -963,6 +969,7 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
 int qsr_observe(qsr_handle* h, const qsr_observe_args* a, qsr_observables* o) {
     clear_error();
     LDG_REQUIRE(h && a && o, LDG_ERR_ARG, "qsr_observe: null argument");
+    DeviceGuard device_guard(h->device);
     const qsr_params& p = h->p;
     ObsConst O{};
     O.P = make_const(h, a->T, a->S_shell, 1.0);
@@ -1055,6 +1062,7 @@ int qsr_observe(qsr_handle* h, const qsr_observe_args* a, qsr_observables* o) {
 int qsr_autotune(qsr_handle* h, const qsr_step_args* a, int trial_steps, int* chosen_chunk) {
     clear_error();
     LDG_REQUIRE(h && a, LDG_ERR_ARG, "qsr_autotune: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(trial_steps >= 1, LDG_ERR_ARG, "qsr_autotune: trial_steps must be >= 1");
     LDG_REQUIRE(h->uploaded, LDG_ERR_STATE, "qsr_autotune: no field uploaded");
     LDG_REQUIRE(h->tiled.ok, LDG_ERR_STATE, "qsr_autotune: no tiled plan");
@@ -1115,6 +1123,7 @@ int qsr_autotune(qsr_handle* h, const qsr_step_args* a, int trial_steps, int* ch
 int qsr_sync(qsr_handle* h) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "qsr_sync: null handle");
+    DeviceGuard device_guard(h->device);
     LDG_CUDA(cudaStreamSynchronize(h->stream));
     return tiled_check(h->tiled, h->stream);
 }
@@ -1125,6 +1134,7 @@ long long qsr_launch_count(const qsr_handle* h) { return h ? h->launches : 0; }
 
 int qsr_destroy(qsr_handle* h) {
     if (!h) return LDG_OK;
+    DeviceGuard device_guard(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->q[0]); cudaFree(h->q[1]); cudaFree(h->lo[0]); cudaFree(h->lo[1]); cudaFree(h->rhs); cudaFree(h->flags);
     if (!h->stage_shared) cudaFree(h->stage);
@@ -1144,6 +1154,7 @@ int qsr_destroy(qsr_handle* h) {
 // ---------------------------------------------------------------------------------------
 struct ens_handle {
     ens_params p{};
+    int device = -1;                       // the GPU the ensemble was created on
     double* stage = nullptr;               // host-boundary staging shared by all droplets
     std::vector<qsr_handle*> inst;
     std::vector<ens_instance> desc;
@@ -1309,6 +1320,7 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
     ens_handle* h = new (std::nothrow) ens_handle();
     LDG_REQUIRE(h, LDG_ERR_NOMEM, "ens_create: host allocation failed");
     h->p = p;
+    cudaGetDevice(&h->device);
     h->desc.assign(instances, instances + n_instances);
     h->L2 = p.L2 != 0.0;
     h->L3 = p.L3 != 0.0;
@@ -1426,6 +1438,7 @@ int ens_create(const ens_params* params, int n_instances, const ens_instance* in
 int ens_initial_fields(ens_handle* h, int init_mode, double S0, double noise_amplitude) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "ens_initial_fields: null handle");
+    DeviceGuard device_guard(h->device);
     LDG_CUDA(cudaStreamSynchronize(h->stream));
     std::vector<double> buf;
     for (size_t n = 0; n < h->inst.size(); ++n) {
@@ -1442,6 +1455,7 @@ int ens_initial_fields(ens_handle* h, int init_mode, double S0, double noise_amp
 int ens_upload(ens_handle* h, int instance, const double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "ens_upload: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_upload: instance out of range");
     LDG_CUDA(cudaStreamSynchronize(h->stream));
     // qsr_upload fills both ping-pong buffers, so either parity of the step index reads it.
@@ -1453,6 +1467,7 @@ int ens_upload(ens_handle* h, int instance, const double* q) {
 int ens_download(ens_handle* h, int instance, double* q) {
     clear_error();
     LDG_REQUIRE(h && q, LDG_ERR_ARG, "ens_download: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_download: instance out of range");
     int rc = ens_check(h);
     if (rc) return rc;
@@ -1463,6 +1478,7 @@ int ens_download(ens_handle* h, int instance, double* q) {
 int ens_nematic(ens_handle* h, int instance, double* s_n) {
     clear_error();
     LDG_REQUIRE(h && s_n, LDG_ERR_ARG, "ens_nematic: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_nematic: instance out of range");
     int rc = ens_check(h);
     if (rc) return rc;
@@ -1473,6 +1489,7 @@ int ens_nematic(ens_handle* h, int instance, double* s_n) {
 int ens_step(ens_handle* h, int n_steps) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "ens_step: null handle");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(n_steps >= 0, LDG_ERR_ARG, "ens_step: n_steps must be >= 0");
     for (qsr_handle* q : h->inst) LDG_REQUIRE(q->uploaded, LDG_ERR_STATE, "ens_step: an instance has no field");
     if (h->n_items == 0) {
@@ -1502,6 +1519,7 @@ int ens_step(ens_handle* h, int n_steps) {
 int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_observables* out) {
     clear_error();
     LDG_REQUIRE(h && out, LDG_ERR_ARG, "ens_observe: null argument");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(instance >= 0 && instance < (int)h->inst.size(), LDG_ERR_ARG, "ens_observe: instance out of range");
     int rc = ens_check(h);
     if (rc) return rc;
@@ -1538,6 +1556,7 @@ int ens_geometry(const ens_handle* h, int instance, qsr_geometry_info* out) {
 int ens_autotune(ens_handle* h, int trial_steps, int* chosen_chunk) {
     clear_error();
     LDG_REQUIRE(h, LDG_ERR_ARG, "ens_autotune: null handle");
+    DeviceGuard device_guard(h->device);
     LDG_REQUIRE(trial_steps >= 1, LDG_ERR_ARG, "ens_autotune: trial_steps must be >= 1");
     for (qsr_handle* q : h->inst) LDG_REQUIRE(q->uploaded, LDG_ERR_STATE, "ens_autotune: an instance has no field");
     LDG_CUDA(cudaStreamSynchronize(h->stream));
@@ -1616,6 +1635,7 @@ long long ens_launch_count(const ens_handle* h) {
 
 int ens_destroy(ens_handle* h) {
     if (!h) return LDG_OK;
+    DeviceGuard device_guard(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     ens_drop_graph(h);
     for (qsr_handle* q : h->inst) qsr_destroy(q);
