@@ -155,7 +155,7 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
             ens2.step(k)
             done += k
         for n, o in enumerate(outs):
-            o[:] = ens2.download(n)
+            ens2.download(n, out=o)
         t_e2e = max_over_ranks(pg, time.perf_counter() - t0)
         ens2.close()
         e2e = {"value": world * c["cells"] * args.steps / t_e2e, "unit": UNIT,

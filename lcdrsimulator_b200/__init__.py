@@ -352,8 +352,12 @@ class EnsembleSolver:
             raise LdgError(f"upload: expected {5 * self.cells(instance)} doubles, got {q.size}")
         _check(load_library().ens_upload(self._h, instance, q.ctypes.data_as(_dp)), "ens_upload")
 
-    def download(self, instance) -> np.ndarray:
-        out = np.empty(5 * self.cells(instance))
+    def download(self, instance, out=None) -> np.ndarray:
+        n = 5 * self.cells(instance)
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise LdgError(f"download: out must be a contiguous float64 array of {n} values")
         _check(load_library().ens_download(self._h, instance, out.ctypes.data_as(_dp)), "ens_download")
         return out
 
