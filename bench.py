@@ -149,8 +149,7 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
         while done < args.steps:
             k = min(w["log_every"], args.steps - done)
             if done % w["log_every"] == 0:
-                for n in range(len(inst)):
-                    ens2.observe(n)
+                ens2.observe_all()
                 n_obs += 1
             ens2.step(k)
             done += k
@@ -161,7 +160,7 @@ def bench_ensemble(args, w, torch, pg, rank, world, local):
         e2e = {"value": world * c["cells"] * args.steps / t_e2e, "unit": UNIT,
                "h2d_bytes_per_step": 40 * c["cells"] / args.steps,
                "d2h_bytes_per_step": (40 * c["cells"] + n_obs * len(inst) * 136) / args.steps,
-               "note": "ens_upload of every droplet + K steps + ens_observe of every droplet every 100 steps + "
+               "note": "ens_upload of every droplet + K steps + ens_observe_all every 100 steps + "
                        "ens_download of every droplet; host wall clock around the whole sequence"}
     if rank == 0:
         line = {"metric": METRIC, "value": world * c["cells"] * args.steps / (ms / 1e3), "unit": UNIT,

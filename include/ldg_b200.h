@@ -181,6 +181,10 @@ int ens_step(ens_handle* h, int n_steps);
 /* Observables of one instance at the current step; args NULL: T and S_shell from the
  * instance's protocol, slices Nz/2, thresholds 0.1 / 0.25. */
 int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_observables* out);
+/* Observables of every instance (out[n_instances]) at the current step in one pass: all
+ * reductions are enqueued on the ensemble's stream and synchronised once. args: NULL for each
+ * instance's defaults (as ens_observe with NULL), else one qsr_observe_args per instance. */
+int ens_observe_all(ens_handle* h, const qsr_observe_args* args, qsr_observables* out);
 long long ens_step_index(const ens_handle* h);
 int ens_geometry(const ens_handle* h, int instance, qsr_geometry_info* out);
 /* Times each candidate work-item length (planes per tile item) for trial_steps steps and keeps

@@ -148,6 +148,7 @@ def load_library():
     L.ens_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
     L.ens_geometry.argtypes = [C.c_void_p, C.c_int, C.POINTER(QsrGeometry)]
     L.ens_nematic.argtypes = [C.c_void_p, C.c_int, _dp]
+    L.ens_observe_all.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.ens_destroy.argtypes = [C.c_void_p]
     for name in ("ens_step_index", "ens_cells", "ens_active_cells", "ens_written_cells", "ens_launch_count"):
         getattr(L, name).restype = C.c_longlong
@@ -379,6 +380,12 @@ class EnsembleSolver:
         g = QsrGeometry()
         _check(load_library().ens_geometry(self._h, instance, C.byref(g)), "ens_geometry")
         return {f[0]: getattr(g, f[0]) for f in g._fields_}
+
+    def observe_all(self) -> list[dict]:
+        """Observables of every droplet at its protocol temperature, in one pass."""
+        out = (QsrObservables * len(self.instances))()
+        _check(load_library().ens_observe_all(self._h, None, out), "ens_observe_all")
+        return [o.as_dict() for o in out]
 
     def autotune(self, trial_steps=10) -> int:
         c = C.c_int(0)

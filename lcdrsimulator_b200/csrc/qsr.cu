@@ -657,6 +657,104 @@ int kernel_choice() {
 
 }  // namespace
 
+namespace {
+
+// Enqueues the observables of the current field on stream `st`, with the block results copied
+// to R and SR (host memory; pinned for the copies to be asynchronous).
+int observe_enqueue(qsr_handle* h, const qsr_observe_args* a, cudaStream_t st, ObsPartial* R, SlicePartial* SR,
+                    bool* wd_out, bool* wx_out) {
+    const qsr_params& p = h->p;
+    ObsConst O{};
+    O.P = make_const(h, a->T, a->S_shell, 1.0);
+    O.i2x = 1.0 / (2.0 * p.dx); O.i2y = 1.0 / (2.0 * p.dy); O.i2z = 1.0 / (2.0 * p.dz);
+    const double dT = a->T - p.T_star;
+    if (p.bulk_modechoice == 1) { O.c2 = (3.0 * p.a * dT) / 2.0; O.c3 = (3.0 * p.b) / 2.0; O.c4 = (9.0 * p.c) / 8.0; }
+    else { O.c2 = (3.0 * p.a * dT) / 2.0; O.c3 = (9.0 * p.b) / 2.0; O.c4 = (9.0 * p.c) / 4.0; }
+    O.all_L_zero = (p.L1 == 0.0 && p.L2 == 0.0 && p.L3 == 0.0);
+    O.Liso = p.kappa; O.L1 = p.L1; O.L2 = p.L2; O.L3 = p.L3;
+    O.dV = p.dx * p.dy * p.dz;
+    O.Weff_half = (h->delta_eff > 0.0) ? 0.5 * (p.W / h->delta_eff) : 0.0;
+    O.S_shell = a->S_shell;
+    O.cx = 0.5 * (p.Nx - 1.0); O.cy = 0.5 * (p.Ny - 1.0); O.cz = 0.5 * (p.Nz - 1.0);
+    // Surface normal ~ (X dx/rx^2, Y dy/ry^2, Z dz/rz^2) in cell units, scaled relative to x.
+    const double sx = p.dx / (h->g.rx * h->g.rx);
+    O.gx = 1.0;
+    O.gy = (p.dy / (h->g.ry * h->g.ry)) / sx;
+    O.gz = (p.dz / (h->g.rz * h->g.rz)) / sx;
+    O.hx = p.dx; O.hy = p.dy; O.hz = p.dz;
+    O.checker_k = std::min(std::max(a->defects_z_slice, 0), p.Nz - 1);
+    const float* q = h->q[h->cur];
+    k_observe_volume<<<kObsBlocks, kObsThreads, 0, st>>>(q, h->flags, O, h->opart);
+    h->launches++;
+    LDG_LAUNCHED("k_observe_volume");
+    k_observe_finalize<<<1, kObsThreads, 0, st>>>(h->opart, kObsBlocks, h->opart + kObsBlocks);
+    h->launches++;
+    LDG_LAUNCHED("k_observe_finalize");
+    const bool wd = a->want_defects && a->defects_z_slice >= 0 && a->defects_z_slice < p.Nz;
+    const bool wx = a->want_xi && a->xi_z_slice >= 0 && a->xi_z_slice < p.Nz;
+    const long long nxy = (long long)p.Nx * p.Ny;
+    if (wd || wx) {
+        double* dnf = h->snf;
+        double* xnf = h->snf + 3 * nxy;
+        if (wd) {
+            k_slice_nematic<<<grid_blocks(nxy, 256, 148 * 4), 256, 0, st>>>(q, O.P, a->defects_z_slice, dnf);
+            h->launches++;
+        }
+        if (wx) {
+            if (wd && a->xi_z_slice == a->defects_z_slice) {
+                xnf = dnf;
+            } else {
+                k_slice_nematic<<<grid_blocks(nxy, 256, 148 * 4), 256, 0, st>>>(q, O.P, a->xi_z_slice, xnf);
+                h->launches++;
+            }
+        }
+        const int mode = (wd ? 1 : 0) | (wx ? 2 : 0);
+        k_slice_metrics<<<kSliceBlocks, kObsThreads, 0, st>>>(dnf, xnf, p.Nx, p.Ny, a->defects_S_threshold,
+                                                                     a->defects_charge_cutoff, a->xi_S_threshold, mode,
+                                                                     h->spart);
+        k_slice_finalize<<<1, kObsThreads, 0, st>>>(h->spart, kSliceBlocks, h->spart + kSliceBlocks);
+        h->launches += 2;
+        LDG_LAUNCHED("k_slice_metrics");
+    }
+    LDG_CUDA(cudaMemcpyAsync(R, h->opart + kObsBlocks, sizeof(*R), cudaMemcpyDeviceToHost, st));
+    if (wd || wx) LDG_CUDA(cudaMemcpyAsync(SR, h->spart + kSliceBlocks, sizeof(*SR), cudaMemcpyDeviceToHost, st));
+    *wd_out = wd;
+    *wx_out = wx;
+    return LDG_OK;
+}
+
+// Fills the observables from the reduced block results.
+void observe_finish(const qsr_handle* h, const ObsPartial& R, const SlicePartial& SR, bool wd, bool wx,
+                    qsr_observables* o) {
+    const qsr_params& p = h->p;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    std::memset(o, 0, sizeof(*o));
+    o->bulk = R.bulk; o->elastic = R.elastic; o->anchoring = R.anch;
+    o->total = R.bulk + R.elastic + R.anch;
+    o->radiality_count = (long long)R.rad_n;
+    o->radiality = R.rad_n > 0 ? R.rad_sum / (double)R.rad_n : 0.0;
+    o->core_count = (long long)R.core_n;
+    o->avg_S = R.core_n > 0 ? R.S_sum / (double)R.core_n : 0.0;
+    o->max_S = R.S_max;
+    o->checker_rel = nan;
+    if (R.S_max >= 0.5 && R.ce_n > 10 && R.co_n > 10 && R.ca_n > 20 && R.ca != 0.0)
+        o->checker_rel = std::fabs(R.ce - R.co) / std::fabs(R.ca);
+    o->defect_count = (long long)SR.defects;
+    o->defect_plaquettes = (long long)SR.plaq;
+    o->defect_density = (wd && SR.plaq > 0) ? (double)SR.defects / (double)SR.plaq : nan;
+    o->xi_edges = (long long)SR.edges;
+    o->xi_grad_proxy = nan;
+    if (wx && SR.edges > 0) {
+        const double ms = SR.xi_sum / (double)SR.edges;
+        const double inv = (ms > 0.0) ? (1.0 / std::sqrt(ms + 1e-30)) : (1.0 / std::sqrt(1e-30));
+        o->xi_grad_proxy = std::min(inv, 0.5 * (double)std::min(p.Nx, p.Ny));
+    }
+    o->max_q_norm = R.qmax;
+    o->nonfinite_cells = (long long)R.nonfinite;
+}
+
+}  // namespace
+
 extern "C" {
 
 int qsr_create(const qsr_params* params, qsr_handle** out) {
@@ -970,92 +1068,14 @@ int qsr_observe(qsr_handle* h, const qsr_observe_args* a, qsr_observables* o) {
     clear_error();
     LDG_REQUIRE(h && a && o, LDG_ERR_ARG, "qsr_observe: null argument");
     DeviceGuard device_guard(h->device);
-    const qsr_params& p = h->p;
-    ObsConst O{};
-    O.P = make_const(h, a->T, a->S_shell, 1.0);
-    O.i2x = 1.0 / (2.0 * p.dx); O.i2y = 1.0 / (2.0 * p.dy); O.i2z = 1.0 / (2.0 * p.dz);
-    const double dT = a->T - p.T_star;
-    if (p.bulk_modechoice == 1) { O.c2 = (3.0 * p.a * dT) / 2.0; O.c3 = (3.0 * p.b) / 2.0; O.c4 = (9.0 * p.c) / 8.0; }
-    else { O.c2 = (3.0 * p.a * dT) / 2.0; O.c3 = (9.0 * p.b) / 2.0; O.c4 = (9.0 * p.c) / 4.0; }
-    O.all_L_zero = (p.L1 == 0.0 && p.L2 == 0.0 && p.L3 == 0.0);
-    O.Liso = p.kappa; O.L1 = p.L1; O.L2 = p.L2; O.L3 = p.L3;
-    O.dV = p.dx * p.dy * p.dz;
-    O.Weff_half = (h->delta_eff > 0.0) ? 0.5 * (p.W / h->delta_eff) : 0.0;
-    O.S_shell = a->S_shell;
-    O.cx = 0.5 * (p.Nx - 1.0); O.cy = 0.5 * (p.Ny - 1.0); O.cz = 0.5 * (p.Nz - 1.0);
-    // Surface normal ~ (X dx/rx^2, Y dy/ry^2, Z dz/rz^2) in cell units, scaled relative to x.
-    const double sx = p.dx / (h->g.rx * h->g.rx);
-    O.gx = 1.0;
-    O.gy = (p.dy / (h->g.ry * h->g.ry)) / sx;
-    O.gz = (p.dz / (h->g.rz * h->g.rz)) / sx;
-    O.hx = p.dx; O.hy = p.dy; O.hz = p.dz;
-    O.checker_k = std::min(std::max(a->defects_z_slice, 0), p.Nz - 1);
-    const float* q = h->q[h->cur];
-    k_observe_volume<<<kObsBlocks, kObsThreads, 0, h->stream>>>(q, h->flags, O, h->opart);
-    h->launches++;
-    LDG_LAUNCHED("k_observe_volume");
-    k_observe_finalize<<<1, kObsThreads, 0, h->stream>>>(h->opart, kObsBlocks, h->opart + kObsBlocks);
-    h->launches++;
-    LDG_LAUNCHED("k_observe_finalize");
-    const bool wd = a->want_defects && a->defects_z_slice >= 0 && a->defects_z_slice < p.Nz;
-    const bool wx = a->want_xi && a->xi_z_slice >= 0 && a->xi_z_slice < p.Nz;
-    const long long nxy = (long long)p.Nx * p.Ny;
-    if (wd || wx) {
-        double* dnf = h->snf;
-        double* xnf = h->snf + 3 * nxy;
-        if (wd) {
-            k_slice_nematic<<<grid_blocks(nxy, 256, 148 * 4), 256, 0, h->stream>>>(q, O.P, a->defects_z_slice, dnf);
-            h->launches++;
-        }
-        if (wx) {
-            if (wd && a->xi_z_slice == a->defects_z_slice) {
-                xnf = dnf;
-            } else {
-                k_slice_nematic<<<grid_blocks(nxy, 256, 148 * 4), 256, 0, h->stream>>>(q, O.P, a->xi_z_slice, xnf);
-                h->launches++;
-            }
-        }
-        const int mode = (wd ? 1 : 0) | (wx ? 2 : 0);
-        k_slice_metrics<<<kSliceBlocks, kObsThreads, 0, h->stream>>>(dnf, xnf, p.Nx, p.Ny, a->defects_S_threshold,
-                                                                     a->defects_charge_cutoff, a->xi_S_threshold, mode,
-                                                                     h->spart);
-        k_slice_finalize<<<1, kObsThreads, 0, h->stream>>>(h->spart, kSliceBlocks, h->spart + kSliceBlocks);
-        h->launches += 2;
-        LDG_LAUNCHED("k_slice_metrics");
-    }
     ObsPartial R{};
     SlicePartial SR{};
-    LDG_CUDA(cudaMemcpyAsync(&R, h->opart + kObsBlocks, sizeof(R), cudaMemcpyDeviceToHost, h->stream));
-    if (wd || wx) LDG_CUDA(cudaMemcpyAsync(&SR, h->spart + kSliceBlocks, sizeof(SR), cudaMemcpyDeviceToHost, h->stream));
+    bool wd = false, wx = false;
+    int rc = observe_enqueue(h, a, h->stream, &R, &SR, &wd, &wx);
+    if (rc) return rc;
     LDG_CUDA(cudaStreamSynchronize(h->stream));
-    {
-        const int rc = tiled_check(h->tiled, h->stream);
-        if (rc) return rc;
-    }
-    const double nan = std::numeric_limits<double>::quiet_NaN();
-    std::memset(o, 0, sizeof(*o));
-    o->bulk = R.bulk; o->elastic = R.elastic; o->anchoring = R.anch;
-    o->total = R.bulk + R.elastic + R.anch;
-    o->radiality_count = (long long)R.rad_n;
-    o->radiality = R.rad_n > 0 ? R.rad_sum / (double)R.rad_n : 0.0;
-    o->core_count = (long long)R.core_n;
-    o->avg_S = R.core_n > 0 ? R.S_sum / (double)R.core_n : 0.0;
-    o->max_S = R.S_max;
-    o->checker_rel = nan;
-    if (R.S_max >= 0.5 && R.ce_n > 10 && R.co_n > 10 && R.ca_n > 20 && R.ca != 0.0)
-        o->checker_rel = std::fabs(R.ce - R.co) / std::fabs(R.ca);
-    o->defect_count = (long long)SR.defects;
-    o->defect_plaquettes = (long long)SR.plaq;
-    o->defect_density = (wd && SR.plaq > 0) ? (double)SR.defects / (double)SR.plaq : nan;
-    o->xi_edges = (long long)SR.edges;
-    o->xi_grad_proxy = nan;
-    if (wx && SR.edges > 0) {
-        const double ms = SR.xi_sum / (double)SR.edges;
-        const double inv = (ms > 0.0) ? (1.0 / std::sqrt(ms + 1e-30)) : (1.0 / std::sqrt(1e-30));
-        o->xi_grad_proxy = std::min(inv, 0.5 * (double)std::min(p.Nx, p.Ny));
-    }
-    o->max_q_norm = R.qmax;
-    o->nonfinite_cells = (long long)R.nonfinite;
+    if ((rc = tiled_check(h->tiled, h->stream))) return rc;
+    observe_finish(h, R, SR, wd, wx, o);
     return LDG_OK;
 }
 
@@ -1156,6 +1176,7 @@ struct ens_handle {
     ens_params p{};
     int device = -1;                       // the GPU the ensemble was created on
     double* stage = nullptr;               // host-boundary staging shared by all droplets
+    void* obs_host = nullptr;              // pinned block results of ens_observe_all
     std::vector<qsr_handle*> inst;
     std::vector<ens_instance> desc;
     std::vector<tiled::EnsInstDev> host_inst;
@@ -1285,6 +1306,25 @@ int ens_check(ens_handle* h) {
 // Makes every instance's current buffer the input of the ensemble's next step.
 void ens_sync_cur(ens_handle* h) {
     for (qsr_handle* q : h->inst) q->cur = (int)(h->step & 1);
+}
+
+// Observables of a droplet at the ensemble's current step: its protocol temperature, its shell
+// order, slices Nz/2, thresholds 0.1 / 0.25.
+qsr_observe_args ens_default_observe_args(const ens_handle* h, int instance) {
+    qsr_observe_args a{};
+    const tiled::EnsInstDev& D = h->host_inst[instance];
+    a.T = tiled::ens_temperature(D, h->step);
+    const double A = D.a3 * (a.T - D.T_star);
+    a.S_shell = D.custom_shell ? D.S_custom : std::max(0.0, tiled::ens_S_eq(A, D.B, D.C));
+    const int Nz = h->inst[instance]->p.Nz;
+    a.defects_z_slice = Nz / 2;
+    a.xi_z_slice = Nz / 2;
+    a.defects_S_threshold = 0.1;
+    a.defects_charge_cutoff = 0.25;
+    a.xi_S_threshold = 0.1;
+    a.want_defects = 1;
+    a.want_xi = 1;
+    return a;
 }
 
 int ens_set_step(ens_handle* h, long long step) {
@@ -1524,24 +1564,40 @@ int ens_observe(ens_handle* h, int instance, const qsr_observe_args* args, qsr_o
     int rc = ens_check(h);
     if (rc) return rc;
     ens_sync_cur(h);
-    qsr_observe_args a{};
-    if (args) {
-        a = *args;
-    } else {
-        const tiled::EnsInstDev& D = h->host_inst[instance];
-        a.T = tiled::ens_temperature(D, h->step);
-        const double A = D.a3 * (a.T - D.T_star);
-        a.S_shell = D.custom_shell ? D.S_custom : std::max(0.0, tiled::ens_S_eq(A, D.B, D.C));
-        const int Nz = h->inst[instance]->p.Nz;
-        a.defects_z_slice = Nz / 2;
-        a.xi_z_slice = Nz / 2;
-        a.defects_S_threshold = 0.1;
-        a.defects_charge_cutoff = 0.25;
-        a.xi_S_threshold = 0.1;
-        a.want_defects = 1;
-        a.want_xi = 1;
-    }
+    const qsr_observe_args a = args ? *args : ens_default_observe_args(h, instance);
     return qsr_observe(h->inst[instance], &a, out);
+}
+
+int ens_observe_all(ens_handle* h, const qsr_observe_args* args, qsr_observables* out) {
+    clear_error();
+    LDG_REQUIRE(h && out, LDG_ERR_ARG, "ens_observe_all: null argument");
+    DeviceGuard device_guard(h->device);
+    int rc = ens_check(h);
+    if (rc) return rc;
+    ens_sync_cur(h);
+    const size_t n = h->inst.size();
+    if (!h->obs_host) {
+        LDG_CUDA(cudaMallocHost((void**)&h->obs_host, n * (sizeof(ObsPartial) + sizeof(SlicePartial))));
+    }
+    ObsPartial* R = reinterpret_cast<ObsPartial*>(h->obs_host);
+    SlicePartial* SR = reinterpret_cast<SlicePartial*>(R + n);
+    std::vector<char> wd(n), wx(n);
+    std::vector<qsr_observe_args> a(n);
+    for (size_t i = 0; i < n; ++i) {
+        a[i] = args ? args[i] : ens_default_observe_args(h, (int)i);
+        std::memset(&SR[i], 0, sizeof(SlicePartial));
+        bool d = false, x = false;
+        // every droplet's reductions on the ensemble's stream, after its steps
+        if ((rc = observe_enqueue(h->inst[i], &a[i], h->stream, &R[i], &SR[i], &d, &x))) return rc;
+        wd[i] = d;
+        wx[i] = x;
+    }
+    LDG_CUDA(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < n; ++i) {
+        if ((rc = tiled_check(h->inst[i]->tiled, h->stream))) return rc;
+        observe_finish(h->inst[i], R[i], SR[i], wd[i] != 0, wx[i] != 0, &out[i]);
+    }
+    return LDG_OK;
 }
 
 long long ens_step_index(const ens_handle* h) { return h ? h->step : -1; }
@@ -1640,6 +1696,7 @@ int ens_destroy(ens_handle* h) {
     ens_drop_graph(h);
     for (qsr_handle* q : h->inst) qsr_destroy(q);
     cudaFree(h->stage);
+    if (h->obs_host) cudaFreeHost(h->obs_host);
     cudaFree(h->d_tms); cudaFree(h->d_inst); cudaFree(h->d_items); cudaFree(h->d_ctl); cudaFree(h->d_err);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

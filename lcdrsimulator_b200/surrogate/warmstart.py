@@ -112,7 +112,7 @@ def relax(cases: list[Case], n: int, dx: float, fields: list[np.ndarray], max_st
     for i, f in enumerate(fields):
         ens.upload(i, np.ascontiguousarray(f, dtype=np.float64).ravel())
     stream = torch.cuda.ExternalStream(ens.stream())
-    energy = [[ens.observe(i)["total"]] for i in range(len(cases))]
+    energy = [[o["total"]] for o in ens.observe_all()]
     conv_step = [None] * len(cases)
     steps = 0
     dev_ms = 0.0
@@ -124,8 +124,9 @@ def relax(cases: list[Case], n: int, dx: float, fields: list[np.ndarray], max_st
         e1.synchronize()
         dev_ms += e0.elapsed_time(e1)
         steps += check_every
+        obs_now = ens.observe_all()
         for i in range(len(cases)):
-            E = ens.observe(i)["total"]
+            E = obs_now[i]["total"]
             if conv_step[i] is None:
                 rate = abs(E - energy[i][-1]) / max(abs(E), 1e-300) / check_every
                 if rate < tol:
@@ -134,7 +135,7 @@ def relax(cases: list[Case], n: int, dx: float, fields: list[np.ndarray], max_st
         if all(s is not None for s in conv_step):
             break
     out = [ens.download(i).reshape(n, n, n, 5) for i in range(len(cases))]
-    obs = [ens.observe(i) for i in range(len(cases))]
+    obs = ens.observe_all()
     ens.close()
     return dict(fields=out, conv_step=conv_step, energy=energy, steps=steps, dt=dt, device_ms=dev_ms, obs=obs)
 

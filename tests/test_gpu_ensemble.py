@@ -215,3 +215,17 @@ def test_ensemble_bad_arguments():
     with pytest.raises(LdgError):
         ens.upload(0, np.zeros(7))
     ens.close()
+
+
+def test_observe_all_matches_per_droplet_observe():
+    p, instances = build("weak_L1L2L3_ramp_custom")
+    ens = EnsembleSolver(instances, **p)
+    ens.initial_fields(init_mode=0, S0=0.5)
+    ens.step(17)
+    every = ens.observe_all()
+    assert len(every) == len(instances)
+    for n in range(len(instances)):
+        one = ens.observe(n)
+        for k, v in one.items():   # checker_rel is NaN when no cell has a checkerboard pattern
+            assert every[n][k] == v or (np.isnan(v) and np.isnan(every[n][k])), (n, k)
+    ens.close()
