@@ -103,17 +103,23 @@ def geometries(cases: list[Case], n: int, dx: float) -> list[dict]:
 
 
 def relax(cases: list[Case], n: int, dx: float, fields: list[np.ndarray], max_steps: int, check_every: int,
-          tol: float, dt: float | None = None) -> dict:
+          tol: float, dt: float | None = None, snapshot_tols=()) -> dict:
     """Relaxes every case from its field (n^3 x 5, FP64) in one ensemble; returns the final
     fields, the first checked step at which each case met the criterion (None if never), the
-    energy histories and the device time of the stepping."""
+    energy histories and the device time of the stepping. For every tolerance in
+    `snapshot_tols` the field of each case is also kept at the first check where its rate fell
+    below that tolerance (`snapshots[t][i]`, step in `snapshot_step[t][i]`; a case that never
+    got there keeps its final field and the last step)."""
     dt = stable_dt(dx, cases) if dt is None else dt
     ens = EnsembleSolver(instances(cases, n, dx), dx=dx, dy=dx, dz=dx, dt=dt, **MATERIAL)
     for i, f in enumerate(fields):
         ens.upload(i, np.ascontiguousarray(f, dtype=np.float64).ravel())
+    chunk = ens.autotune()   # small droplets want short work items; the fields are restored
     stream = torch.cuda.ExternalStream(ens.stream())
     energy = [[o["total"]] for o in ens.observe_all()]
     conv_step = [None] * len(cases)
+    snaps = {t: [None] * len(cases) for t in snapshot_tols}
+    snap_step = {t: [None] * len(cases) for t in snapshot_tols}
     steps = 0
     dev_ms = 0.0
     while steps < max_steps:
@@ -127,17 +133,25 @@ def relax(cases: list[Case], n: int, dx: float, fields: list[np.ndarray], max_st
         obs_now = ens.observe_all()
         for i in range(len(cases)):
             E = obs_now[i]["total"]
-            if conv_step[i] is None:
-                rate = abs(E - energy[i][-1]) / max(abs(E), 1e-300) / check_every
-                if rate < tol:
-                    conv_step[i] = steps
+            rate = abs(E - energy[i][-1]) / max(abs(E), 1e-300) / check_every
+            if conv_step[i] is None and rate < tol:
+                conv_step[i] = steps
+            for t in snapshot_tols:
+                if snaps[t][i] is None and rate < t:
+                    snaps[t][i] = ens.download(i).reshape(n, n, n, 5)
+                    snap_step[t][i] = steps
             energy[i].append(E)
         if all(s is not None for s in conv_step):
             break
     out = [ens.download(i).reshape(n, n, n, 5) for i in range(len(cases))]
     obs = ens.observe_all()
     ens.close()
-    return dict(fields=out, conv_step=conv_step, energy=energy, steps=steps, dt=dt, device_ms=dev_ms, obs=obs)
+    for t in snapshot_tols:
+        for i in range(len(cases)):
+            if snaps[t][i] is None:
+                snaps[t][i], snap_step[t][i] = out[i], steps
+    return dict(fields=out, conv_step=conv_step, energy=energy, steps=steps, dt=dt, device_ms=dev_ms, obs=obs,
+                snapshots=snaps, snapshot_step=snap_step, chunk=chunk)
 
 
 # ---------------------------------------------------------------------------------------
@@ -191,11 +205,25 @@ def cube_symmetry(x: torch.Tensor, perm, flips, q_slices):
     return y.contiguous()
 
 
+def masked_loss(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, batch: int = 8) -> float:
+    """The training loss (masked MSE on the 5 scaled Q components) over a data set, no gradients."""
+    tot, cnt = 0.0, 0.0
+    with torch.no_grad():
+        for s in range(0, len(inputs), batch):
+            X = torch.from_numpy(inputs[s:s + batch]).to("cuda", torch.bfloat16)
+            Y = torch.from_numpy(targets[s:s + batch] * Q_SCALE).to("cuda", torch.float32)
+            M = torch.from_numpy(masks[s:s + batch].astype(np.float32)).to("cuda")[..., None]
+            tot += float((((net(X)[..., :5] - Y) ** 2) * M).sum())
+            cnt += float(M.sum()) * 5
+    return tot / max(cnt, 1.0)
+
+
 def train(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, epochs: int = 40, batch: int = 8,
-          lr: float = 1e-3, seed: int = 0, log=None, augment: bool = False) -> list[float]:
-    """Masked MSE on the 5 scaled Q components; Adam with gradient clipping and cosine decay;
-    each batch transformed by a random cube symmetry when `augment` (at 512 training droplets
-    and 80 epochs this under-fits: 2.0x instead of 2.55x time-to-equilibrium speed-up)."""
+          lr: float = 1e-3, seed: int = 0, log=None, augment: bool = False, warmup_epochs: float = 0.0) -> list[float]:
+    """Masked MSE on the 5 scaled Q components; Adam with gradient clipping, a linear learning-rate
+    warm-up over `warmup_epochs` and cosine decay after it; each batch transformed by a random
+    cube symmetry when `augment` (at 512 training droplets and 80 epochs this under-fits: 2.0x
+    instead of 2.55x time-to-equilibrium speed-up)."""
     dev = torch.device("cuda")
     X = torch.from_numpy(inputs).to(dev, torch.bfloat16)
     Y = torch.from_numpy(targets * Q_SCALE).to(dev, torch.float32)
@@ -203,7 +231,14 @@ def train(net, inputs: np.ndarray, targets: np.ndarray, masks: np.ndarray, epoch
     n = X.shape[0]
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     total = epochs * ((n + batch - 1) // batch)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, total)
+    warm = int(round(warmup_epochs * ((n + batch - 1) // batch)))
+
+    def lr_factor(step):
+        if step < warm:
+            return (step + 1) / warm
+        return 0.5 * (1.0 + math.cos(math.pi * (step - warm) / max(total - warm, 1)))
+
+    sched = torch.optim.lr_scheduler.LambdaLR(opt, lr_factor)
     g = torch.Generator().manual_seed(seed)
     hist = []
     for ep in range(epochs):
@@ -271,41 +306,87 @@ def make_dataset(cases: list[Case], n_coarse: int, dx_fine: float, max_steps: in
     return dict(X=np.stack(X), Y=np.stack(Y), M=np.stack(Mk), conv=conv)
 
 
+def _geomean(xs):
+    xs = [x for x in xs if x]
+    return float(np.exp(np.mean(np.log(xs)))) if xs else None
+
+
 def evaluate(net, cases: list[Case], n_coarse: int, dx_fine: float, max_steps: int, check_every: int, tol: float,
-             log=None) -> dict:
+             log=None, coarse_tols=(), coarse_max_steps: int = 600000) -> dict:
     """Plain relaxation from the fine low-pass field against relaxation from the upsampled
-    prediction, all cases and both arms in one ensemble with one dt."""
+    prediction, all cases and all arms in one ensemble with one dt.
+
+    With `coarse_tols`, two more arms per tolerance t run a coarse stage first (both on the
+    n_coarse grid, same dt): "unet+coarse@t" relaxes the network's prediction and "coarse@t"
+    (the control without the network) relaxes the 2x2x2 average of the fine initial field, each
+    until its rate per step falls below t; the upsampled coarse field then starts a fine
+    relaxation to `tol`. Cost of an arm = coarse steps x device time per coarse droplet-step +
+    fine steps x device time per fine droplet-step (both measured here, in ensembles of the same
+    kind); its speed-up is the plain arm's cost over that."""
     nf = 2 * n_coarse
     dxc = 2.0 * dx_fine
     gcs = geometries(cases, n_coarse, dxc)
     gfs = geometries(cases, nf, dx_fine)
-    fine0, inputs, warm = [], [], []
+    fine0, inputs, warm, mfs, mcs = [], [], [], [], []
     for c, gc, gf in zip(cases, gcs, gfs):
         mf = droplet_mask(gf, nf, dx_fine)
         mc = droplet_mask(gc, n_coarse, dxc)
         q = lowpass_field(nf, c.seed) * mf[..., None]
         fine0.append(q)
+        mfs.append(mf)
+        mcs.append(mc)
         inputs.append(network_input(pool2(q) * mc[..., None], mc, c))
     t0 = time.perf_counter()
     pred = predict(net, np.stack(inputs))
     torch.cuda.synchronize()
     t_pred = time.perf_counter() - t0
-    for p, gf in zip(pred, gfs):
-        warm.append(upsample2(p) * droplet_mask(gf, nf, dx_fine)[..., None])
-    both = cases + cases
+    for p, mf in zip(pred, mfs):
+        warm.append(upsample2(p) * mf[..., None])
     dt = stable_dt(dx_fine, cases)
-    r = relax(both, nf, dx_fine, fine0 + warm, max_steps, check_every, tol, dt=dt)
     k = len(cases)
+    arms = {"plain": fine0, "unet": warm}
+    coarse = {}
+    if coarse_tols:
+        starts = [p * mc[..., None] for p, mc in zip(pred, mcs)] + \
+                 [pool2(q) * mc[..., None] for q, mc in zip(fine0, mcs)]
+        rc = relax(cases + cases, n_coarse, dxc, starts, coarse_max_steps, check_every, min(coarse_tols), dt=dt,
+                   snapshot_tols=tuple(coarse_tols))
+        coarse["us_per_droplet_step"] = rc["device_ms"] * 1e3 / max(rc["steps"], 1) / (2 * k)
+        coarse["steps"] = rc["steps"]
+        coarse["chunk"] = rc["chunk"]
+        for t in coarse_tols:
+            for a, name in enumerate((f"unet+coarse@{t:g}", f"coarse@{t:g}")):
+                arms[name] = [upsample2(rc["snapshots"][t][a * k + i]) * mfs[i][..., None] for i in range(k)]
+                coarse[name] = [rc["snapshot_step"][t][a * k + i] for i in range(k)]
+    names = list(arms)
+    r = relax(cases * len(names), nf, dx_fine, [f for nm in names for f in arms[nm]], max_steps, check_every, tol,
+              dt=dt)
+    t_f = r["device_ms"] * 1e3 / max(r["steps"], 1) / (len(names) * k)
+    t_c = coarse.get("us_per_droplet_step", 0.0)
     res = []
     for i, c in enumerate(cases):
-        sp, sw = r["conv_step"][i], r["conv_step"][k + i]
-        op, ow = r["obs"][i], r["obs"][k + i]
-        res.append(dict(case=dataclasses.asdict(c), plain_steps=sp, warm_steps=sw,
-                        plain_E=op["total"], warm_E=ow["total"],
-                        plain_defects=op["defect_count"], warm_defects=ow["defect_count"],
-                        plain_E0=r["energy"][i][0], warm_E0=r["energy"][k + i][0]))
+        row = dict(case=dataclasses.asdict(c), arms={})
+        for a, nm in enumerate(names):
+            j = a * k + i
+            fs = r["conv_step"][j]
+            cs = coarse[nm][i] if nm in coarse else 0
+            row["arms"][nm] = dict(coarse_steps=cs, fine_steps=fs, E=r["obs"][j]["total"], E0=r["energy"][j][0],
+                                   defects=r["obs"][j]["defect_count"],
+                                   cost_us=(cs * t_c + fs * t_f) if fs is not None else None)
+        base = row["arms"]["plain"]["cost_us"]
+        for nm in names:
+            cu = row["arms"][nm]["cost_us"]
+            row["arms"][nm]["speedup"] = base / cu if (base and cu) else None
+        # fields kept for the plain/warm summary
+        row.update(plain_steps=row["arms"]["plain"]["fine_steps"], warm_steps=row["arms"]["unet"]["fine_steps"],
+                   plain_E=row["arms"]["plain"]["E"], warm_E=row["arms"]["unet"]["E"],
+                   plain_defects=row["arms"]["plain"]["defects"], warm_defects=row["arms"]["unet"]["defects"],
+                   plain_E0=row["arms"]["plain"]["E0"], warm_E0=row["arms"]["unet"]["E0"])
+        res.append(row)
         if log:
-            log(f"case {i}: plain {sp} steps E={op['total']:.6e}, warm {sw} steps E={ow['total']:.6e}")
-    return dict(results=res, dt=dt, steps=r["steps"], device_ms=r["device_ms"], predict_s=t_pred,
-                step_us_per_instance=r["device_ms"] * 1e3 / max(r["steps"], 1) / len(both),
+            log(f"case {i}: " + ", ".join(f"{nm} {row['arms'][nm]['coarse_steps']}+{row['arms'][nm]['fine_steps']} "
+                                          f"x{row['arms'][nm]['speedup'] or 0:.2f}" for nm in names))
+    summary = {nm: _geomean([row["arms"][nm]["speedup"] for row in res]) for nm in names}
+    return dict(results=res, dt=dt, steps=r["steps"], device_ms=r["device_ms"], predict_s=t_pred, chunk=r["chunk"],
+                step_us_per_instance=t_f, coarse=coarse, arms=names, speedup_geomean_by_arm=summary,
                 energy_plain=[r["energy"][i] for i in range(k)], energy_warm=[r["energy"][k + i] for i in range(k)])
