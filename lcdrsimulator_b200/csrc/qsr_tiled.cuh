@@ -192,36 +192,34 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     const bool tile_interior = (j0 >= 2) && (j0 + TJ + 2 <= P.Ny) && (k0 >= 2) && (k0 + TK + 2 <= P.Nz);
     // Column divergence of plane p on the tile plus a 1-cell halo into D slot p % NDS.
     // Reads Q planes p-1 .. p+1 (all waited for by the caller).
+    // Work split: warp w computes columns 0..31 of D rows w, w + 8, ... (a warp never spans two
+    // rows, so its shared-memory accesses are bank-conflict free); the two remaining columns of
+    // every row (2 x DROWS cells) go to the warp that has one row fewer, DROWS % 8.
+    static_assert(DRW == 32 + 2 && 2 * DROWS <= 32, "D tile = 32 + 2 columns, one spare warp");
+    constexpr int NWARP = THREADS / 32, SPARE = DROWS % NWARP;
     auto compute_D = [&](int p) {
         if (p < 0 || p >= P.Nx) return;
         float* dst = sd + ((p + NDS) % NDS) * DPLANE;
         SmemQ A;
 #pragma unroll
         for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(p + d - 2, base)) * PLANE;
-        if (tile_interior && p >= 1 && p <= P.Nx - 2) {
-            for (int t = tid; t < DROWS * DRW; t += THREADS) {
-                const int r = t / DRW, cidx = t - r * DRW;
-                float D[3];
-                A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
-                dcol_at<false>(A, P, p, j0 + r - 1, k0 + cidx - 1, 0, 0, 0, D);
-                dst[t] = D[0];
-                dst[DCSTR + t] = D[1];
-                dst[2 * DCSTR + t] = D[2];
-            }
-            return;
-        }
-        for (int t = tid; t < DROWS * DRW; t += THREADS) {
-            const int r = t / DRW, cidx = t - r * DRW;
+        const int lane = tid & 31, warp = tid >> 5;
+        const bool face_free = tile_interior && p >= 1 && p <= P.Nx - 2;
+        auto one = [&](int r, int cidx) {
+            const int t = r * DRW + cidx;
             const int j = j0 + r - 1, k = k0 + cidx - 1;
             float D[3] = {0.0f, 0.0f, 0.0f};
-            if (j >= 0 && j < P.Ny && k >= 0 && k < P.Nz) {
-                A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
+            A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
+            if (face_free)
+                dcol_at<false>(A, P, p, j, k, 0, 0, 0, D);
+            else if (j >= 0 && j < P.Ny && k >= 0 && k < P.Nz)
                 dcol_at(A, P, p, j, k, 0, 0, 0, D);
-            }
             dst[t] = D[0];
             dst[DCSTR + t] = D[1];
             dst[2 * DCSTR + t] = D[2];
-        }
+        };
+        for (int r = warp; r < DROWS; r += NWARP) one(r, lane);
+        if (warp == SPARE && lane < 2 * DROWS) one(lane >> 1, 32 + (lane & 1));
     };
 
     // Prologue: planes ib-2 .. ib+LOOK-1, then D(ib-1) .. D(ib+1) (visible after the barrier).
