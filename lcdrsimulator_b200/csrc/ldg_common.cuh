@@ -46,6 +46,11 @@ struct QsrConst {
     // semi-implicit (IMEX) Helmholtz-Jacobi
     float alpha;                // (dt/gamma) L_stab
     float jdenom_inv;           // 1/(1 + 2 alpha sum 1/d^2)
+    // products of the constants above, folded on the host so the interior stencils need one
+    // fused multiply-add per term
+    float lap_c;                // -2 (1/dx^2 + 1/dy^2 + 1/dz^2): centre weight of the Laplacian
+    float L2i2x, L2i2y, L2i2z;  // L2/(2d)
+    float l3m[6];               // (L3/2) / (4 da db) for M_ab from undivided central differences (xx yy zz xy xz yz)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -153,13 +158,14 @@ __device__ __forceinline__ void bulk_field(const float q[5], float cQ, float cQ2
     const float q2yz = Qxy * Qxz + Qyy * Qyz + Qyz * Qzz;
     const float q2zz = Qxz * Qxz + Qyz * Qyz + Qzz * Qzz;
     const float t3 = trQ2 * (1.0f / 3.0f);  // FP32 path: reciprocal multiply (one rounding)
-    const float g = cQ3 * trQ2;
-    h[0] = cQ * Qxx - cQ2 * (q2xx - t3) + g * Qxx;
-    h[1] = cQ * Qyy - cQ2 * (q2yy - t3) + g * Qyy;
-    h[2] = cQ * Qzz - cQ2 * (q2zz - t3) + g * Qzz;
-    h[3] = cQ * Qxy - cQ2 * q2xy + g * Qxy;
-    h[4] = cQ * Qxz - cQ2 * q2xz + g * Qxz;
-    h[5] = cQ * Qyz - cQ2 * q2yz + g * Qyz;
+    // cQ Q - cQ2 (Q^2 - tr/3) + cQ3 tr(Q^2) Q with the two linear terms joined: (cQ + cQ3 tr) Q
+    const float cg = fmaf(cQ3, trQ2, cQ);
+    h[0] = fmaf(-cQ2, q2xx - t3, cg * Qxx);
+    h[1] = fmaf(-cQ2, q2yy - t3, cg * Qyy);
+    h[2] = fmaf(-cQ2, q2zz - t3, cg * Qzz);
+    h[3] = fmaf(-cQ2, q2xy, cg * Qxy);
+    h[4] = fmaf(-cQ2, q2xz, cg * Qxz);
+    h[5] = fmaf(-cQ2, q2yz, cg * Qyz);
 }
 
 // Droplet surface normal at cell (i, j, k) (QSR.cu:130-142), in FP32 from cell units.
@@ -186,10 +192,18 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
                                                const float q[5], bool anchor, float mu[5], float lap[5]) {
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-        const float d2x = d2_face<0, kFaces>(A, c, q[c], i, P.Nx, P.ix2);
-        const float d2y = d2_face<1, kFaces>(A, c, q[c], j, P.Ny, P.iy2);
-        const float d2z = d2_face<2, kFaces>(A, c, q[c], k, P.Nz, P.iz2);
-        lap[c] = d2x + d2y + d2z;
+        if (!kFaces) {
+            // interior: sum_a (Q[+1] + Q[-1]) / da^2 - 2 Q sum_a 1/da^2
+            const float sx = A(c, 1, 0, 0) + A(c, -1, 0, 0);
+            const float sy = A(c, 0, 1, 0) + A(c, 0, -1, 0);
+            const float sz = A(c, 0, 0, 1) + A(c, 0, 0, -1);
+            lap[c] = fmaf(P.ix2, sx, fmaf(P.iy2, sy, fmaf(P.iz2, sz, P.lap_c * q[c])));
+        } else {
+            const float d2x = d2_face<0, kFaces>(A, c, q[c], i, P.Nx, P.ix2);
+            const float d2y = d2_face<1, kFaces>(A, c, q[c], j, P.Ny, P.iy2);
+            const float d2z = d2_face<2, kFaces>(A, c, q[c], k, P.Nz, P.iz2);
+            lap[c] = d2x + d2y + d2z;
+        }
     }
     float h[6];
     bulk_field(q, P.cQ, P.cQ2, P.cQ3, h);
@@ -201,26 +215,28 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
     h[4] -= P.Liso * lap[2];
     h[5] -= P.Liso * lap[4];
     if (kL2) {
-        // d_a D_b with one-sided faces (QSR.cu:436-460).
-        auto dD = [&](int comp, int ax) {
+        // h -= L2 d_a D_b, d_a central with one-sided faces (QSR.cu:436-460). sub() applies one
+        // term as a fused multiply-add with L2/(2 da) (central) or L2/da = 2 L2/(2 da) (one-sided).
+        auto sub = [&](float& hv, int comp, int ax) {
             const int pos = ax == 0 ? i : (ax == 1 ? j : k);
             const int n = ax == 0 ? P.Nx : (ax == 1 ? P.Ny : P.Nz);
-            const float i2 = ax == 0 ? P.i2x : (ax == 1 ? P.i2y : P.i2z);
-            const float i1 = ax == 0 ? P.ix : (ax == 1 ? P.iy : P.iz);
+            const float c2 = ax == 0 ? P.L2i2x : (ax == 1 ? P.L2i2y : P.L2i2z);
             auto at = [&](int s) {
                 return ax == 0 ? DA(comp, s, 0, 0) : (ax == 1 ? DA(comp, 0, s, 0) : DA(comp, 0, 0, s));
             };
-            if (!kFaces || (pos > 0 && pos < n - 1)) return (at(1) - at(-1)) * i2;
-            if (pos == 0) return (at(1) - at(0)) * i1;
-            return (at(0) - at(-1)) * i1;
+            if (!kFaces || (pos > 0 && pos < n - 1)) hv = fmaf(-c2, at(1) - at(-1), hv);
+            else if (pos == 0) hv = fmaf(-2.0f * c2, at(1) - at(0), hv);
+            else hv = fmaf(-2.0f * c2, at(0) - at(-1), hv);
         };
-        const float L2 = P.L2;
-        h[0] -= L2 * dD(0, 0);
-        h[1] -= L2 * dD(1, 1);
-        h[2] -= L2 * dD(2, 2);
-        h[3] -= L2 * (dD(1, 0) + dD(0, 1));
-        h[4] -= L2 * (dD(2, 0) + dD(0, 2));
-        h[5] -= L2 * (dD(2, 1) + dD(1, 2));
+        sub(h[0], 0, 0);
+        sub(h[1], 1, 1);
+        sub(h[2], 2, 2);
+        sub(h[3], 1, 0);
+        sub(h[3], 0, 1);
+        sub(h[4], 2, 0);
+        sub(h[4], 0, 2);
+        sub(h[5], 2, 1);
+        sub(h[5], 1, 2);
     }
     float corr = (h[0] + h[1] + h[2]) * (1.0f / 3.0f);
     mu[0] = h[0] - corr;
@@ -233,12 +249,14 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
             !kFaces || (i > 0 && i < P.Nx - 1 && j > 0 && j < P.Ny - 1 && k > 0 && k < P.Nz - 1);
         if (interior) {
             float hx[6] = {mu[0], mu[3], -(mu[0] + mu[3]), mu[1], mu[2], mu[4]};
+            // undivided central differences Q[+1] - Q[-1]; the 1/(2 da) factors are folded into
+            // the M_ab weights (P.l3m) and into the divergence below
             float d[6][3];
 #pragma unroll
             for (int c = 0; c < 5; ++c) {
-                d[c][0] = (A(c, 1, 0, 0) - A(c, -1, 0, 0)) * P.i2x;
-                d[c][1] = (A(c, 0, 1, 0) - A(c, 0, -1, 0)) * P.i2y;
-                d[c][2] = (A(c, 0, 0, 1) - A(c, 0, 0, -1)) * P.i2z;
+                d[c][0] = A(c, 1, 0, 0) - A(c, -1, 0, 0);
+                d[c][1] = A(c, 0, 1, 0) - A(c, 0, -1, 0);
+                d[c][2] = A(c, 0, 0, 1) - A(c, 0, 0, -1);
             }
 #pragma unroll
             for (int a = 0; a < 3; ++a) d[5][a] = -(d[0][a] + d[3][a]);
@@ -246,29 +264,29 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
                 return d[0][a] * d[0][b] + d[3][a] * d[3][b] + d[5][a] * d[5][b] +
                        2.0f * (d[1][a] * d[1][b] + d[2][a] * d[2][b] + d[4][a] * d[4][b]);
             };
-            const float hl3 = 0.5f * P.L3;
-            hx[0] += hl3 * M(0, 0);
-            hx[1] += hl3 * M(1, 1);
-            hx[2] += hl3 * M(2, 2);
-            hx[3] += hl3 * M(0, 1);
-            hx[4] += hl3 * M(0, 2);
-            hx[5] += hl3 * M(1, 2);
+            hx[0] = fmaf(P.l3m[0], M(0, 0), hx[0]);
+            hx[1] = fmaf(P.l3m[1], M(1, 1), hx[1]);
+            hx[2] = fmaf(P.l3m[2], M(2, 2), hx[2]);
+            hx[3] = fmaf(P.l3m[3], M(0, 1), hx[3]);
+            hx[4] = fmaf(P.l3m[4], M(0, 2), hx[4]);
+            hx[5] = fmaf(P.l3m[5], M(1, 2), hx[5]);
             const float Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4], Qzz = -q[0] - q[3];
-            const float Dc0 = DA(0, 0, 0, 0), Dc1 = DA(1, 0, 0, 0), Dc2 = DA(2, 0, 0, 0);
+            // D_a / (2 da): pairs with the undivided differences in D . grad Q_c
+            const float Dc0 = DA(0, 0, 0, 0) * P.i2x, Dc1 = DA(1, 0, 0, 0) * P.i2y, Dc2 = DA(2, 0, 0, 0) * P.i2z;
             // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603), with the Q_ab / (stencil
             // denominator) weights formed once for all five components.
             const float wxx = Qxx * P.ix2, wyy = Qyy * P.iy2, wzz = Qzz * P.iz2;
             const float wxy = 2.0f * Qxy * P.i4xy, wxz = 2.0f * Qxz * P.i4xz, wyz = 2.0f * Qyz * P.i4yz;
             auto Bc = [&](int c) {
                 const float Qc2 = 2.0f * (c == 5 ? Qzz : q[c]);
-                const float sxx = A(c, 1, 0, 0) - Qc2 + A(c, -1, 0, 0);
-                const float syy = A(c, 0, 1, 0) - Qc2 + A(c, 0, -1, 0);
-                const float szz = A(c, 0, 0, 1) - Qc2 + A(c, 0, 0, -1);
+                const float sxx = (A(c, 1, 0, 0) + A(c, -1, 0, 0)) - Qc2;
+                const float syy = (A(c, 0, 1, 0) + A(c, 0, -1, 0)) - Qc2;
+                const float szz = (A(c, 0, 0, 1) + A(c, 0, 0, -1)) - Qc2;
                 const float sxy = (A(c, 1, 1, 0) - A(c, 1, -1, 0)) - (A(c, -1, 1, 0) - A(c, -1, -1, 0));
                 const float sxz = (A(c, 1, 0, 1) - A(c, 1, 0, -1)) - (A(c, -1, 0, 1) - A(c, -1, 0, -1));
                 const float syz = (A(c, 0, 1, 1) - A(c, 0, 1, -1)) - (A(c, 0, -1, 1) - A(c, 0, -1, -1));
                 const float contract = wxx * sxx + wyy * syy + wzz * szz + wxy * sxy + wxz * sxz + wyz * syz;
-                return Dc0 * d[c][0] + Dc1 * d[c][1] + Dc2 * d[c][2] + contract;
+                return fmaf(Dc0, d[c][0], fmaf(Dc1, d[c][1], fmaf(Dc2, d[c][2], contract)));
             };
             const float Bxx = Bc(0), Byy = Bc(3), Bzz = -(Bxx + Byy);
             const float Bxy = Bc(1), Bxz = Bc(2), Byz = Bc(4);

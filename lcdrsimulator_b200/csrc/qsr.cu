@@ -610,6 +610,12 @@ QsrConst make_const(const qsr_handle* h, double T, double S_shell, double dt) {
     P.gnx = 1.0f;
     P.gny = (float)((p.dy / (h->g.ry * h->g.ry)) / sxn);
     P.gnz = (float)((p.dz / (h->g.rz * h->g.rz)) / sxn);
+    const double ix2 = 1.0 / (p.dx * p.dx), iy2 = 1.0 / (p.dy * p.dy), iz2 = 1.0 / (p.dz * p.dz);
+    P.lap_c = (float)(-2.0 * (ix2 + iy2 + iz2));
+    P.L2i2x = (float)(p.L2 / (2.0 * p.dx)); P.L2i2y = (float)(p.L2 / (2.0 * p.dy)); P.L2i2z = (float)(p.L2 / (2.0 * p.dz));
+    const double i2[3] = {1.0 / (2.0 * p.dx), 1.0 / (2.0 * p.dy), 1.0 / (2.0 * p.dz)};
+    const int ab[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+    for (int m = 0; m < 6; ++m) P.l3m[m] = (float)(0.5 * p.L3 * i2[ab[m][0]] * i2[ab[m][1]]);
     return P;
 }
 
