@@ -158,8 +158,9 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 
     // Plane p (p >= base) lives in slot (p - base) % NQ and completes that slot's barrier phase
     // number (p - base) / NQ of this item.
-    auto slot = [&](int p) { return (p - base) % NQ; };
-    auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (uint32_t)(((p - base) / NQ) & 1); };
+    // (every caller has p >= base, so the ring arithmetic is unsigned: a mask and a shift)
+    auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
+    auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
 
     // Planes outside the grid complete their phase with a plain arrive (no data).
     auto issue = [&](int p) {
@@ -197,12 +198,12 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     // every row (2 x DROWS cells) go to the warp that has one row fewer, DROWS % 8.
     static_assert(DRW == 32 + 2 && 2 * DROWS <= 32, "D tile = 32 + 2 columns, one spare warp");
     constexpr int NWARP = THREADS / 32, SPARE = DROWS % NWARP;
-    auto compute_D = [&](int p) {
+    // pm, pc, pp: the shared-memory Q planes p-1, p, p+1 (the first derivatives reach no
+    // further); dst: the D slot of plane p.
+    auto compute_D = [&](int p, const float* pm, const float* pc, const float* pp, float* dst) {
         if (p < 0 || p >= P.Nx) return;
-        float* dst = sd + ((p + NDS) % NDS) * DPLANE;
         SmemQ A;
-#pragma unroll
-        for (int d = 0; d < 5; ++d) A.pl[d] = sq + slot(max(p + d - 2, base)) * PLANE;
+        A.pl[0] = pm; A.pl[1] = pm; A.pl[2] = pc; A.pl[3] = pp; A.pl[4] = pp;
         const int lane = tid & 31, warp = tid >> 5;
         const bool face_free = tile_interior && p >= 1 && p <= P.Nx - 2;
         auto one = [&](int r, int cidx) {
@@ -225,10 +226,10 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     // Prologue: planes ib-2 .. ib+LOOK-1, then D(ib-1) .. D(ib+1) (visible after the barrier).
     for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     __syncthreads();
+    auto qplane = [&](int p) { return sq + slot(p) * PLANE; };
+    auto dslot = [&](int p) { return sd + ((uint32_t)(p + NDS) % (uint32_t)NDS) * DPLANE; };
     if (kD && !*S.s_abort) {
-        compute_D(ib - 1);
-        compute_D(ib);
-        compute_D(ib + 1);
+        for (int p = ib - 1; p <= ib + 1; ++p) compute_D(p, qplane(p - 1), qplane(p), qplane(p + 1), dslot(p));
     }
     __syncthreads();
 
@@ -241,13 +242,15 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     const long long cell0 = (long long)j * P.sj + k;
     uint8_t f_next = in_grid ? __ldg(flags + (long long)ib * P.si + cell0) : 0;
     // Shared-memory planes of the current step, rolled forward by one plane per step:
-    // Q planes i-2 .. i+2 and divergence planes i-1 .. i+1.
-    const float* qpl[5];
-    const float* dpl[3];
+    // Q planes i-2 .. i+3 (the cells read i-2 .. i+2, D(i+2) reads i+1 .. i+3) and divergence
+    // slots i-1 .. i+2 (the cells read i-1 .. i+1, D(i+2) is written; the four slots rotate).
+    const float* qpl[6];
+    float* dpl[NDS];
+    static_assert(NDS == 4, "divergence slots i-1 .. i+2");
 #pragma unroll
-    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+    for (int d = 0; d < 6; ++d) qpl[d] = qplane(ib + d - 2);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) dpl[d] = sd + ((ib + d - 1 + NDS) % NDS) * DPLANE;
+    for (int d = 0; d < NDS; ++d) dpl[d] = dslot(ib + d - 1);
     // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
     // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
     for (int i = ib; i < ie; ++i) {
@@ -255,7 +258,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         const uint8_t f = f_next;
         if (in_grid && i + 1 < ie) f_next = __ldg(flags + (long long)(i + 1) * P.si + cell0);
         wait_plane(i + LOOK);
-        if (kD) compute_D(i + 2);
+        if (kD) compute_D(i + 2, qpl[3], qpl[4], qpl[5], dpl[3]);
         const bool fixed = in_grid && !kRHS && (f & kFixed);
         const bool move = in_grid && (f & kMove) != 0;
         // The face-free form is taken by a whole warp when none of its computing cells touches a
@@ -321,11 +324,13 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         }
         ++issued_end;
 #pragma unroll
-        for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
-        qpl[4] = sq + slot(i + 3) * PLANE;
+        for (int d = 0; d < 5; ++d) qpl[d] = qpl[d + 1];
+        qpl[5] = qplane(i + 4);
+        float* const d0 = dpl[0];  // slot of D(i-1) takes D(i+3)
         dpl[0] = dpl[1];
         dpl[1] = dpl[2];
-        dpl[2] = sd + ((i + 2 + NDS) % NDS) * DPLANE;
+        dpl[2] = dpl[3];
+        dpl[3] = d0;
     }
     // Drain: every load this item issued lands before the slots are reused or released.
     for (int p = waited_end; p < issued_end; ++p) {
