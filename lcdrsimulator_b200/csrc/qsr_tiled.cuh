@@ -162,10 +162,11 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
     auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
 
-    // Planes outside the grid complete their phase with a plain arrive (no data).
+    // Planes outside the grid, and planes past the last one this item reads (ie - 1 + LOOK),
+    // complete their phase with a plain arrive (no data).
     auto issue = [&](int p) {
         uint64_t* b = &bar[slot(p)];
-        if (p >= 0 && p < P.Nx) {
+        if (p >= 0 && p < P.Nx && p < ie + LOOK) {
             mbar_expect_tx(b, PLANE_BYTES);
             tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
@@ -327,10 +328,9 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         for (int d = 0; d < 5; ++d) qpl[d] = qpl[d + 1];
         qpl[5] = qplane(i + 4);
         float* const d0 = dpl[0];  // slot of D(i-1) takes D(i+3)
-        dpl[0] = dpl[1];
-        dpl[1] = dpl[2];
-        dpl[2] = dpl[3];
-        dpl[3] = d0;
+#pragma unroll
+        for (int d = 0; d < NDS - 1; ++d) dpl[d] = dpl[d + 1];
+        dpl[NDS - 1] = d0;
     }
     // Drain: every load this item issued lands before the slots are reused or released.
     for (int p = waited_end; p < issued_end; ++p) {
