@@ -26,6 +26,7 @@ struct KzmConst {
     long long sz;    // plane pitch
     long long sc;    // component pitch
     float ix2, iy2, iz2;
+    float lap_c;     // -2 (1/dx^2 + 1/dy^2 + 1/dz^2): centre weight of the Laplacian
     float A, B, C, kappa, mob_dt, qcap, sigma;
     uint32_t key0, key1;
     long long step;
@@ -53,9 +54,9 @@ __global__ void __launch_bounds__(256) k_kzm_step(const float* __restrict__ q, f
     for (int m = 0; m < 5; ++m) {
         const float* b = q + m * P.sc;
         c[m] = __ldg(b + id);
-        lap[m] = (__ldg(b + oxp) - 2.0f * c[m] + __ldg(b + oxm)) * P.ix2 +
-                 (__ldg(b + oyp) - 2.0f * c[m] + __ldg(b + oym)) * P.iy2 +
-                 (__ldg(b + ozp) - 2.0f * c[m] + __ldg(b + ozm)) * P.iz2;
+        lap[m] = fmaf(P.ix2, __ldg(b + oxp) + __ldg(b + oxm),
+                      fmaf(P.iy2, __ldg(b + oyp) + __ldg(b + oym),
+                           fmaf(P.iz2, __ldg(b + ozp) + __ldg(b + ozm), P.lap_c * c[m])));
     }
     float h[6];
     bulk_field(c, P.A, P.B, P.C, h);
@@ -149,9 +150,9 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_tiled(const float* __rest
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
                 const float c = qc[m];
-                lap[m] = (s[m][ty + 1][tx + 2] - 2.0f * c + s[m][ty + 1][tx]) * P.ix2 +
-                         (s[m][ty + 2][tx + 1] - 2.0f * c + s[m][ty][tx + 1]) * P.iy2 +
-                         (qp[m] - 2.0f * c + qm[m]) * P.iz2;
+                lap[m] = fmaf(P.ix2, s[m][ty + 1][tx + 2] + s[m][ty + 1][tx],
+                              fmaf(P.iy2, s[m][ty + 2][tx + 1] + s[m][ty][tx + 1],
+                                   fmaf(P.iz2, qp[m] + qm[m], P.lap_c * c)));
             }
             float h[6];
             bulk_field(qc, P.A, P.B, P.C, h);
@@ -266,8 +267,10 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_async(const float* __rest
             for (int m = 0; m < 5; ++m) {
                 const float* s = pc + m * KPS + s_c;
                 c[m] = s[0];
-                lap[m] = (s[1] - 2.0f * c[m] + s[-1]) * P.ix2 + (s[KTX + 2] - 2.0f * c[m] + s[-(KTX + 2)]) * P.iy2 +
-                         (pp[m * KPS + s_c] - 2.0f * c[m] + pm[m * KPS + s_c]) * P.iz2;
+                // sum_a (Q[+1] + Q[-1]) / da^2 - 2 Q sum_a 1/da^2 as one fused chain
+                lap[m] = fmaf(P.ix2, s[1] + s[-1],
+                              fmaf(P.iy2, s[KTX + 2] + s[-(KTX + 2)],
+                                   fmaf(P.iz2, pp[m * KPS + s_c] + pm[m * KPS + s_c], P.lap_c * c[m])));
             }
             float h[6];
             bulk_field(c, P.A, P.B, P.C, h);
@@ -634,6 +637,7 @@ int kzm_create(const kzm_params* params, kzm_handle** out) {
     P.sz = (long long)p.Ny * P.sy;
     P.sc = (long long)p.Nz * P.sz;
     P.ix2 = (float)(1.0 / (p.dx * p.dx)); P.iy2 = (float)(1.0 / (p.dy * p.dy)); P.iz2 = (float)(1.0 / (p.dz * p.dz));
+    P.lap_c = (float)(-2.0 * (1.0 / (p.dx * p.dx) + 1.0 / (p.dy * p.dy) + 1.0 / (p.dz * p.dz)));
     P.kappa = (float)p.kappa;
     P.qcap = (float)p.q_norm_cap;
     h->n = (long long)p.Nx * p.Ny * p.Nz;
