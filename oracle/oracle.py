@@ -286,6 +286,13 @@ class RefCUDA:
                               C.c_int(int(imex)), C.c_double(L_stab), C.c_int(jacobi_iters))
         assert rc == 0
 
+    def time_steps(self, T, S_shell, dt, n):
+        """Device time (ms) of n explicit steps of the reference chain launched back to back."""
+        ms = C.c_float(0.0)
+        rc = self.L.qref_time_steps(C.c_double(T), C.c_double(S_shell), C.c_double(dt), C.c_int(n), C.byref(ms))
+        assert rc == 0, rc
+        return ms.value
+
     def observe(self, T, S_shell, dz_slice, dS_thr=0.1, d_cut=0.25, xi_slice=None, xi_thr=None):
         xi_slice = dz_slice if xi_slice is None else xi_slice
         xi_thr = dS_thr if xi_thr is None else xi_thr

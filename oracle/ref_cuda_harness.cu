@@ -86,8 +86,11 @@ int qref_download(double* q) {
     return cudaMemcpy(q, S.Q, S.n * sizeof(QTensor), cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : 1;
 }
 
-// One step of the reference chain. imex != 0 selects the semi-implicit branch (QSR.cu:2721-2749).
-int qref_step(double T, double S_shell, double dt, double q_norm_cap, int imex, double L_stab, int jacobi_iters) {
+}  // extern "C"
+
+namespace {
+// The kernels of one step of the reference chain, in its launch order, without a synchronisation.
+void launch_step(double T, double S_shell, double dt, double q_norm_cap, int imex, double L_stab, int jacobi_iters) {
     DimensionalParams P = S.P;
     P.T = T;
     const int Nx = S.Nx, Ny = S.Ny, Nz = S.Nz;
@@ -115,7 +118,30 @@ int qref_step(double T, double S_shell, double dt, double q_norm_cap, int imex, 
         updateQTensorKernel<<<grd(), blk()>>>(S.Q, S.mu, Nx, Ny, Nz, dt, S.shell, S.gamma, P.W, q_norm_cap);
     }
     applyBoundaryConditionsKernel<<<grd(), blk()>>>(S.Q, Nx, Ny, Nz, S.shell, S_shell, P.W);
+}
+}  // namespace
+
+extern "C" {
+
+// One step of the reference chain. imex != 0 selects the semi-implicit branch (QSR.cu:2721-2749).
+int qref_step(double T, double S_shell, double dt, double q_norm_cap, int imex, double L_stab, int jacobi_iters) {
+    launch_step(T, S_shell, dt, q_norm_cap, imex, L_stab, jacobi_iters);
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
+// n explicit steps of the reference chain back to back (as its time loop launches them between
+// log points), timed with CUDA events on the default stream: *ms = elapsed device time.
+int qref_time_steps(double T, double S_shell, double dt, int n, float* ms) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return 1;
+    cudaEventRecord(e0);
+    for (int s = 0; s < n; ++s) launch_step(T, S_shell, dt, 0.0, 0, 0.0, 0);
+    cudaEventRecord(e1);
+    const bool ok = cudaEventSynchronize(e1) == cudaSuccess;
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ok && cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 // Observables as the reference's log path computes them (QSR.cu:2323-2410, 2787-2874).

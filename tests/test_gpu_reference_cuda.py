@@ -70,3 +70,59 @@ def test_fused_fp32_tracks_reference_cuda(oracle, refcuda, name):
     so = solver.observe(T, S_shell)
     assert so["total"] == pytest.approx(ro["bulk"] + ro["elastic"] + ro["anchoring"], rel=1e-5)
     solver.close()
+
+
+# Step time of the fused FP32 path against the reference's FP64 kernel chain on the same GPU.
+# The default benchmark workload (256^3, droplet R = 120 cells, L1/L2/L3 = 6/3/1e-12 N,
+# W = 1e-5 J/m^2, boundary_S = 0.6, T = 302 K) and the plain strong-anchoring relaxation of a
+# 64^3 grid (R = 28 cells, L1 only, T = 300 K), both from the reference's seeded random directors.
+TIMING = {
+    "anisotropic_weak_256": (dict(Nx=256, Ny=256, Nz=256, kappa=0.0, L1=6e-12, L2=3e-12, L3=1e-12, W=1e-5,
+                                  droplet_radius_cells=120.0), 302.0, 0.6, 50, 5),
+    "plain_relaxation_64": (dict(Nx=64, Ny=64, Nz=64, kappa=0.0, L1=6e-12, droplet_radius_cells=28.0), 300.0, None,
+                            400, 100),
+}
+
+
+@pytest.mark.parametrize("name", list(TIMING))
+def test_step_time_against_reference_cuda_chain(refcuda, name):
+    import json
+    import os
+    import torch
+    kw, T, S, n_ours, n_ref = TIMING[name]
+    op, solver, d = make_pair(**kw)
+    S_shell = S if S is not None else S_eq(*bulk_ABC(d["a"], d["b"], d["c"], T, d["T_star"]))
+    dt = 1.5e-10
+    q0 = solver.initial_field(0, 42, 0.5)
+    solver.upload(q0)
+    solver.autotune(T, S_shell, dt, trial_steps=5)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    args = solver.step_args(T, S_shell, dt)
+    for s in range(3):
+        args.step_index = s
+        solver.step_raw(1, args)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(n_ours):
+        args.step_index = 3 + s
+        solver.step_raw(1, args)
+    e1.record(stream)
+    e1.synchronize()
+    ours = e0.elapsed_time(e1) / n_ours
+    assert np.isfinite(solver.download()).all()
+    solver.close()
+    refcuda.create(op)
+    refcuda.upload(q0)
+    refcuda.time_steps(T, S_shell, dt, 2)  # warm-up
+    ref = refcuda.time_steps(T, S_shell, dt, n_ref) / n_ref
+    refcuda.destroy()
+    cells = d["Nx"] * d["Ny"] * d["Nz"]
+    rec = dict(workload=name, cells=cells, ours_ms_per_step=ours, reference_cuda_ms_per_step=ref,
+               ours_cell_updates_per_s=cells / (ours * 1e-3), reference_cell_updates_per_s=cells / (ref * 1e-3),
+               speedup=ref / ours)
+    out = os.environ.get("LDG_REF_TIMING_OUT")
+    if out:
+        with open(f"{out}.{name}", "w") as f:
+            json.dump(rec, f)
+    # one fused FP32 launch per step against the reference's seven FP64 kernels per step
+    assert ours * 3.0 < ref, rec
