@@ -329,6 +329,15 @@ class RefKZM:
         assert rc == 0
         return out
 
+    def time_steps(self, bp, q, n_warm, n_steps, A, B, Cc, noise_sigma=0.0, seed=0):
+        """Device time (ms) of n_steps reference updates launched back to back."""
+        ms = C.c_float(0.0)
+        rc = self.L.kref_time(_ptr(self._arr(bp)), _ptr(np.ascontiguousarray(q)), C.c_int(n_warm), C.c_int(n_steps),
+                              C.c_double(A), C.c_double(B), C.c_double(Cc), C.c_double(noise_sigma),
+                              C.c_ulonglong(seed), C.byref(ms))
+        assert rc == 0, rc
+        return ms.value
+
     def observe(self, bp, q, A, B, Cc):
         out = np.zeros(10)
         self.L.kref_observe(_ptr(self._arr(bp)), _ptr(np.ascontiguousarray(q)), C.c_double(A), C.c_double(B),

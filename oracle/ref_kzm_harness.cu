@@ -42,6 +42,36 @@ int kref_run(const double* p, const double* q_in, double* q_out, int n_steps, do
     return e == cudaSuccess ? 0 : 1;
 }
 
+// Device time (*ms) of n_steps reference updates launched back to back after n_warm untimed
+// ones, with CUDA events on the default stream (the reference's time loop, KZM_bulk_ldg.cu:951-970).
+int kref_time(const double* p, const double* q_in, int n_warm, int n_steps, double A, double B, double C,
+              double noise_sigma, unsigned long long seed, float* ms) {
+    const BulkLdgParams b = make(p);
+    const size_t n = (size_t)b.Nx * b.Ny * b.Nz;
+    QTensor *cur = nullptr, *nxt = nullptr;
+    if (cudaMalloc(&cur, n * sizeof(QTensor)) != cudaSuccess) return 1;
+    if (cudaMalloc(&nxt, n * sizeof(QTensor)) != cudaSuccess) { cudaFree(cur); return 1; }
+    cudaMemcpy(cur, q_in, n * sizeof(QTensor), cudaMemcpyHostToDevice);
+    const int bs = 256;
+    const int gs = (int)((n + bs - 1) / bs);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int s = 0; s < n_warm + n_steps; ++s) {
+        if (s == n_warm) cudaEventRecord(e0);
+        updateBulkLdgKernel<<<gs, bs>>>(cur, nxt, b, A, B, C, noise_sigma, seed, s);
+        std::swap(cur, nxt);
+    }
+    cudaEventRecord(e1);
+    const bool ok = cudaEventSynchronize(e1) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(cur);
+    cudaFree(nxt);
+    return ok ? 0 : 2;
+}
+
 // out: bulk elastic total avg_S max_S defect_density line_density xi plaquettes_used defects
 void kref_observe(const double* p, const double* q, double A, double B, double C, double* out) {
     const BulkLdgParams b = make(p);

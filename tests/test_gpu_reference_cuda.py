@@ -126,3 +126,46 @@ def test_step_time_against_reference_cuda_chain(refcuda, name):
             json.dump(rec, f)
     # one fused FP32 launch per step against the reference's seven FP64 kernels per step
     assert ours * 3.0 < ref, rec
+
+
+def test_periodic_step_time_against_reference_kernel():
+    """The periodic quench step (256^3 box, kappa = 6e-12 N, T = 300 K, Langevin noise kT/dx^3)
+    against the reference's FP64 update kernel (KZM_bulk_ldg.cu) on the same GPU and input."""
+    import json
+    import math
+    import os
+    import torch
+    from oracle.oracle import OrcBulkParams, RefKZM
+    from lcdrsimulator_b200 import KZMSolver
+    try:
+        ref = RefKZM()
+    except FileNotFoundError:
+        pytest.skip("reference CUDA build (oracle/_ref/kzm_cuda_ref.so) not available")
+    N, D, KAPPA, GAMMA, DT = 256, 1e-8, 6e-12, 0.1, 1.6e-9
+    A, B, Cc = bulk_ABC(0.044e6, 1.413e6, 1.153e6, 300.0, 307.0)
+    sigma = math.sqrt(2.0 * (1.0 / GAMMA) * (1.380649e-23 * 300.0 / D ** 3) * DT)
+    q0 = np.random.default_rng(5).normal(0.0, 1e-3, N * N * N * 5)
+    s = KZMSolver(N, N, N, D, D, D, KAPPA, GAMMA)
+    s.upload(q0)
+    stream = torch.cuda.ExternalStream(s.stream())
+    s.step(3, A, B, Cc, DT, noise_sigma=sigma, seed=9, step_index=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 50
+    e0.record(stream)
+    s.step(n, A, B, Cc, DT, noise_sigma=sigma, seed=9, step_index=3)
+    e1.record(stream)
+    e1.synchronize()
+    ours = e0.elapsed_time(e1) / n
+    assert np.isfinite(s.download()).all()
+    s.close()
+    bp = OrcBulkParams(N, N, N, D, D, D, KAPPA, GAMMA, DT, 0.0, 0.1, 0.25)
+    theirs = ref.time_steps(bp, q0, 3, 20, A, B, Cc, noise_sigma=sigma, seed=9) / 20
+    sites = N ** 3
+    rec = dict(workload="periodic_quench_256", cells=sites, ours_ms_per_step=ours, reference_cuda_ms_per_step=theirs,
+               ours_cell_updates_per_s=sites / (ours * 1e-3), reference_cell_updates_per_s=sites / (theirs * 1e-3),
+               speedup=theirs / ours)
+    out = os.environ.get("LDG_REF_TIMING_OUT")
+    if out:
+        with open(f"{out}.periodic_quench_256", "w") as f:
+            json.dump(rec, f)
+    assert ours * 2.0 < theirs, rec
