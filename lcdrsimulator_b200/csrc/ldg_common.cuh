@@ -88,16 +88,21 @@ __device__ __forceinline__ void normals5(uint32_t cell, uint32_t instance, long 
     // angle 2 pi u taken as pi + t with t = 2 pi u - pi in (-pi, pi], where the fast hardware
     // sine/cosine is accurate to ~4e-7: cos(2 pi u) = -cos t, sin(2 pi u) = -sin t
     constexpr float kTwoPi = 6.28318530717958647692f, kPi = 3.14159265358979323846f;
+    // radius sqrt(-2 ln u) as t * rsqrt(t) (2 ulp; the guard keeps t = 0, i.e. u = 1, at zero)
+    auto radius = [](float u) {
+        const float t = -2.0f * logf(u);
+        return t * rsqrtf(fmaxf(t, 1e-30f));
+    };
     float s, co;
-    float r = sqrtf(-2.0f * logf(u21(f0)));
+    float r = radius(u21(f0));
     __sincosf(fmaf(kTwoPi, u21(f1), -kPi), &s, &co);
     g[0] = -r * co;
     g[1] = -r * s;
-    r = sqrtf(-2.0f * logf(u21(f2)));
+    r = radius(u21(f2));
     __sincosf(fmaf(kTwoPi, u21(f3), -kPi), &s, &co);
     g[2] = -r * co;
     g[3] = -r * s;
-    r = sqrtf(-2.0f * logf(u21(f4)));
+    r = radius(u21(f4));
     g[4] = -r * __cosf(fmaf(kTwoPi, u21(f5), -kPi));
 }
 
