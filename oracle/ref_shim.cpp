@@ -1,5 +1,6 @@
 // Plain-pointer wrappers around the reference's own CPU functions (QSR.cpp), compiled
-// together with /root/reference/QSR.cpp by oracle/Makefile into oracle/_ref/.
+// together with the reference's QSR.cpp (from the reference tree named by the Makefile's REF)
+// by oracle/Makefile into oracle/_ref/.
 // TEST INFRASTRUCTURE ONLY: used by tests to pin the FP64 oracle's per-cell math to the
 // reference implementation. The reference's main() is renamed at compile time.
 #include "QSR.h"
