@@ -27,3 +27,13 @@ def test_reference_arm_prints_contract_line():
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["config"]["workload"] == "anisotropic_weak_256"
+
+
+def test_l2_note_follows_the_field_size():
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import bench
+    # 256^3 and 512^3 fields (20 B per cell) exceed the 126 MB L2 twice over; 64^3 fits
+    assert bench.l2_note(20 * 256 ** 3).startswith("inputs larger than L2")
+    assert bench.l2_note(20 * 512 ** 3).startswith("inputs larger than L2")
+    assert bench.l2_note(20 * 64 ** 3).startswith("inputs fit in L2")
