@@ -314,11 +314,11 @@ L2_BYTES = 126 * 1024 * 1024
 
 
 def l2_note(field_bytes):
-    """How the timed steps stand against the 126 MB L2: each step reads one 5-component FP32
-    field and writes the other."""
+    """How the timed steps stand against the 126 MB L2: each step reads one field (5 FP32
+    components per cell, or 10 with compensated hi + lo storage) and writes the other."""
     if 2 * field_bytes > L2_BYTES:
-        return "inputs larger than L2 (two 5-component FP32 fields of %.0f MB)" % (field_bytes / 1e6)
-    return "inputs fit in L2 (two 5-component FP32 fields of %.1f MB): not an HBM measurement" % (field_bytes / 1e6)
+        return "inputs larger than L2 (two fields of %.0f MB)" % (field_bytes / 1e6)
+    return "inputs fit in L2 (two fields of %.1f MB): not an HBM measurement" % (field_bytes / 1e6)
 
 
 def load_traffic(workload, alg_bytes):
@@ -406,24 +406,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_sample(w, target_s=12.0, grid=128, max_steps=400):
-    """The reference's own CPU step chain (QSR.cpp) on a bounded sample of the workload."""
-    from oracle.oracle import RefCPU, make_params
-    ref = RefCPU()
+def _reference_problem(w, grid=0):
+    """The workload's own grid, droplet and seeded initial field for the reference's CPU path:
+    parameters, the reference's initial field (initializeQTensor, QSR.cu:1841-1880, from the
+    reference build) and the step scalars. grid > 0 shrinks the box (CPU tests only)."""
+    from oracle.oracle import make_params, ref_initial_field
     p = dict(w["params"])
-    p.update(Nx=grid, Ny=grid, Nz=grid, droplet_radius_cells=0.0)
+    if grid:
+        scale = grid / p["Nx"]
+        p.update(Nx=grid, Ny=grid, Nz=grid, droplet_radius_cells=p.get("droplet_radius_cells", 0.0) * scale)
     op = make_params(**p)
-    rng = np.random.default_rng(w["seed"])
-    q = rng.normal(0.0, 0.2, grid ** 3 * 5)
-    dt = dt_max(w)
-    S_shell = shell_order(w)
+    q = ref_initial_field(op, 0, w["seed"], w["S0"])
+    return op, q, dt_max(w), shell_order(w)
+
+
+def cpu_reference_sample(w, target_s=12.0, max_steps=400):
+    """The reference's own CPU step chain (QSR.cpp) on a bounded number of steps of the workload."""
+    from oracle.oracle import RefCPU
+    ref = RefCPU()
+    op, q, dt, S_shell = _reference_problem(w)
     t1 = ref.run_steps(op, q, w["T"], S_shell, dt, 1)  # warm-up and per-step estimate
     n = int(max(2, min(max_steps, target_s / max(t1, 1e-6))))
     t = ref.run_steps(op, q, w["T"], S_shell, dt, n)
-    cells = grid ** 3
+    cells = op.Nx * op.Ny * op.Nz
     return {"value": cells * n / t, "unit": UNIT, "cores": ref.max_threads(), "kind": "reference",
             "sample": f"QSR.cpp step chain (computeLaplacian, computeChemicalPotential, applyWeakAnchoringPenalty, "
-                      f"updateQTensor, applyBoundaryConditions) on {grid}^3 with the workload's physics, "
+                      f"updateQTensor, applyBoundaryConditions) on the workload's {op.Nx}x{op.Ny}x{op.Nz} grid, "
+                      f"droplet R = {op.droplet_radius_cells:g} cells and seeded initial field, "
                       f"{n} steps, {t:.2f} s"}, t / n
 
 
@@ -432,28 +441,26 @@ def run_reference_arm(args, w):
     if rank != 0:
         return 0
     from oracle.oracle import RefCPU
-    grid = args.ref_grid
-    cells = grid ** 3
-    from oracle.oracle import make_params
     ref = RefCPU()
-    p = dict(w["params"])
-    p.update(Nx=grid, Ny=grid, Nz=grid, droplet_radius_cells=0.0)
-    op = make_params(**p)
-    q = np.random.default_rng(w["seed"]).normal(0.0, 0.2, cells * 5)
-    dt = dt_max(w)
-    S_shell = shell_order(w)
+    op, q, dt, S_shell = _reference_problem(w, args.ref_grid)
+    cells = op.Nx * op.Ny * op.Nz
     if args.warmup > 0:
         ref.run_steps(op, q, w["T"], S_shell, dt, args.warmup)
     t = ref.run_steps(op, q, w["T"], S_shell, dt, args.steps)
     value = cells * args.steps / t
+    same = not args.ref_grid
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": args.workload, "desc": w["desc"], "sample_grid": [grid] * 3,
-                       "note": "the reference CPU path (QSR.cpp) on a bounded sample of the workload"},
+            "config": {"workload": args.workload, "desc": w["desc"], "grid": [op.Nx, op.Ny, op.Nz],
+                       "droplet_radius_cells": op.droplet_radius_cells,
+                       "note": "the reference CPU path (QSR.cpp step chain, all host threads) on "
+                               + ("the workload's own grid, droplet and seeded initial field" if same else
+                                  "a reduced grid of the workload's physics")},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.max_threads(), "kind": "reference",
-                             "sample": f"{grid}^3 grid with the workload's physics, {args.steps} timed steps"},
+                             "sample": f"{op.Nx}^3 grid, droplet R = {op.droplet_radius_cells:g} cells, "
+                                       f"{args.steps} timed steps"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -466,14 +473,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
-    ap.add_argument("--ref-grid", type=int, default=128)
+    ap.add_argument("--ref-grid", type=int, default=0,
+                    help="reference arm: box edge of a reduced grid (0 = the workload's own grid)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--compensated", action="store_true",
                     help="confined workloads: compensated (hi + lo) field storage")
     ap.add_argument("--droplets", type=int, default=0,
                     help="ensemble workload: first N droplets of the distribution (small profiling cases)")
-    ap.add_argument("--grid", type=int, default=0, help="periodic workload: box edge (small profiling cases)")
+    ap.add_argument("--grid", type=int, default=0,
+                    help="box edge of a smaller case of the workload (profiling; droplet radius scaled with it)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -495,6 +504,11 @@ def main():
     if w.get("kind") == "ensemble":
         return bench_ensemble(args, w, torch, pg, rank, world, local)
 
+    if args.grid:
+        # a smaller box of the same physics (profiling cases): droplet radius scaled with the box
+        scale = args.grid / w["params"]["Nx"]
+        w = dict(w, params=dict(w["params"], Nx=args.grid, Ny=args.grid, Nz=args.grid,
+                                droplet_radius_cells=w["params"]["droplet_radius_cells"] * scale))
     solver = L.QSRSolver(**dict(w["params"], compensated=1 if args.compensated else 0))
     geo = solver.geometry()
     q0 = solver.initial_field(0, w["seed"], w["S0"])
@@ -560,7 +574,7 @@ def main():
         alg_bytes += imex["jacobi"] * 60 * box
     achieved = alg_bytes / t_step / 1e9
     # the committed DRAM traffic was captured with plain FP32 storage
-    traffic = None if args.compensated else load_traffic(args.workload, alg_bytes)
+    traffic = None if (args.compensated or args.grid) else load_traffic(args.workload, alg_bytes)
 
     e2e = None
     if not args.no_e2e:
@@ -611,7 +625,7 @@ def main():
                        "active_cell_updates_per_s": world * touched * args.steps / (ms / 1e3),
                        "dt_s": dt, "S_shell": S_shell, "parallelism": f"replicas{world}",
                        "storage": "compensated hi+lo FP32" if args.compensated else "FP32", "chunk": chunk,
-                       "l2": l2_note(20 * box)},
+                       "l2": l2_note((40 if args.compensated else 20) * box)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "bytes_per_launch": alg_bytes, "read_cells": touched, "written_cells": written,

@@ -261,14 +261,18 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* args);
 int kzm_observe(kzm_handle* h, double A, double B, double C, kzm_observables* out);
 /* No counterpart in the reference. The observables of kzm_observe computed straight from a
  * field the caller keeps in device memory (the reference's own layout: AoS FP64, 5 doubles per
- * site, x fastest), for callers that must not allocate device memory: code running under
- * another framework's memory pool, or a loop that is being captured into a CUDA graph. It
- * calls no cudaMalloc/cudaFree: its scratch is a fixed file-scope device array in this
- * library, sized for at most KZM_NOALLOC_MAX_SITES sites (larger grids get LDG_ERR_ARG).
- * The first call on each device looks up that array's device address, so make that first
- * call before any stream capture. All calls share the array: calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialised by the caller. Work runs
- * on `stream` (a cudaStream_t, NULL = legacy default stream); the call synchronises it. */
+ * site, x fastest), for callers that must not allocate device memory: code running inside
+ * another framework that has reserved the GPU's memory for its own pool (a cudaMalloc there can
+ * fail, or take memory the pool expects to own), and step loops that cannot afford the device
+ * synchronisation that cudaMalloc/cudaFree imply. It calls no cudaMalloc/cudaFree: its scratch
+ * is a fixed file-scope device array in this library (16 MiB, held on every GPU that loads the
+ * library until the process exits), sized for at most KZM_NOALLOC_MAX_SITES sites (larger grids
+ * get LDG_ERR_ARG before any device work). The first call on each device looks up that array's
+ * device address, so make that first call before any stream capture. All calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. Work runs on `stream` (a cudaStream_t of the current device,
+ * NULL = legacy default stream; a stream of another device gets LDG_ERR_ARG); the call
+ * synchronises it before returning the observables. */
 #define KZM_NOALLOC_MAX_SITES (1LL << 19)
 int kzm_observe_device_noalloc(const kzm_params* params, const double* q_aos5_device, double A, double B,
                                double C, void* stream, kzm_observables* out);

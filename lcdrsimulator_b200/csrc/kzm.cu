@@ -827,11 +827,20 @@ int kzm_observe_device_noalloc(const kzm_params* params, const double* q, double
     LDG_REQUIRE(n <= KZM_NOALLOC_MAX_SITES, LDG_ERR_ARG,
                 "kzm_observe_device_noalloc: " + std::to_string(n) + " sites exceed the no-allocation scratch limit of " +
                     std::to_string(KZM_NOALLOC_MAX_SITES) + " sites (use kzm_observe for larger grids)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (st) {
+        // the scratch address is the current device's: a stream of another device cannot use it
+        int cur = 0, sdev = 0;
+        LDG_CUDA(cudaGetDevice(&cur));
+        LDG_CUDA(cudaStreamGetDevice(st, &sdev));
+        LDG_REQUIRE(sdev == cur, LDG_ERR_ARG,
+                    "kzm_observe_device_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                        ", not to the current device " + std::to_string(cur));
+    }
     double4* nf = nullptr;
     KzmPartial* part = nullptr;
     int rc = noalloc_scratch(&nf, &part);
     if (rc) return rc;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     KzmObsConst O{};
     O.P.Nx = p.Nx; O.P.Ny = p.Ny; O.P.Nz = p.Nz;
     O.A = A; O.B = B; O.C = C; O.kappa = p.kappa;

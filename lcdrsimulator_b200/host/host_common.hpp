@@ -139,6 +139,69 @@ inline double equilibrium_shell_order(double a, double b, double c, double T, do
     return s > 0.0 ? s : 0.0;
 }
 
+// Shell order of a step: the custom value, or the equilibrium order max(S_eq(T), 0)
+// (resolve_boundary_shell_order, QSR.cu:1475-1487).
+inline double resolve_shell_order(bool custom, double custom_S, double a, double b, double c, double T, double Ts,
+                                  int mode) {
+    return custom ? custom_S : equilibrium_shell_order(a, b, c, T, Ts, mode);
+}
+
+struct DtResult {
+    double min_dx, S_scale, L_eff_total, D_total, dt_diff_total, L_eff_explicit, dt_diff, bulk_rate, dt_bulk, dt_max;
+    bool semi_implicit_active;
+};
+
+// estimate_stable_dt_window (QSR.cu:1528-1604).
+inline DtResult estimate_dt(double dx, double dy, double dz, double gamma, double a, double b, double c, double Ts,
+                     int mode, double kappa, double L1, double L2, double L3, double S_ref_used, double S0, double Ta,
+                     double Tb, bool semi, double L_stab, int jacobi) {
+    DtResult o{};
+    o.min_dx = std::min({dx, dy, dz});
+    o.S_scale = std::isfinite(S_ref_used) ? std::abs(S_ref_used) : std::max(std::abs(S0), 0.5);
+    const double sa = std::abs(equilibrium_shell_order(a, b, c, Ta, Ts, mode));
+    const double sb = std::abs(equilibrium_shell_order(a, b, c, Tb, Ts, mode));
+    if (std::isfinite(sa) && sa > 0.0) o.S_scale = std::max(o.S_scale, sa);
+    if (std::isfinite(sb) && sb > 0.0) o.S_scale = std::max(o.S_scale, sb);
+    o.S_scale = std::max(o.S_scale, 1.0);
+    const bool ldg = (L1 != 0.0 || L2 != 0.0 || L3 != 0.0);
+    const bool aniso = (L2 != 0.0 || L3 != 0.0);
+    o.L_eff_total = ldg ? std::max({std::abs(L1), std::abs(L2), std::abs(L1 + L2), std::abs(L1 + 2.0 * L2),
+                                    std::abs(L3) * o.S_scale})
+                        : std::abs(kappa);
+    if (!(o.L_eff_total > 0.0)) o.L_eff_total = 1e-12;
+    o.D_total = o.L_eff_total / gamma;
+    if (!(o.D_total > 0.0) || !std::isfinite(o.D_total)) o.D_total = 1e-12;
+    o.dt_diff_total = 0.5 * (o.min_dx * o.min_dx) / (6.0 * o.D_total);
+    if (aniso) o.dt_diff_total *= 0.25;
+    o.L_eff_explicit = o.L_eff_total;
+    o.dt_diff = o.dt_diff_total;
+    if (semi && L_stab > 0.0 && jacobi > 0) {
+        const double L_base = ldg ? L1 : kappa;
+        const double Ls = (L_base >= 0.0) ? L_stab : -L_stab;
+        const double L_rem = std::abs(L_base - Ls);
+        o.L_eff_explicit = ldg ? std::max({L_rem, std::abs(L2), std::abs(L1 + L2), std::abs(L1 + 2.0 * L2),
+                                           std::abs(L3) * o.S_scale})
+                               : L_rem;
+        if (o.L_eff_explicit > 0.0) {
+            o.dt_diff = 0.5 * (o.min_dx * o.min_dx) / (6.0 * (o.L_eff_explicit / gamma));
+            if (aniso) o.dt_diff *= 0.25;
+        } else {
+            o.dt_diff = std::numeric_limits<double>::infinity();
+        }
+        o.semi_implicit_active = true;
+    }
+    auto rate = [&](double T) {
+        double A, B, C;
+        bulk_ABC(a, b, c, T, Ts, mode, A, B, C);
+        return std::abs(A) + std::abs(B) * o.S_scale + std::abs(C) * o.S_scale * o.S_scale;
+    };
+    o.bulk_rate = std::max(rate(Ta), rate(Tb));
+    o.dt_bulk = (o.bulk_rate > 0.0) ? (0.02 * gamma / o.bulk_rate) : std::numeric_limits<double>::infinity();
+    o.dt_max = std::min(o.dt_diff, o.dt_bulk);
+    if (!(o.dt_max > 0.0) || !std::isfinite(o.dt_max)) o.dt_max = o.dt_diff;
+    return o;
+}
+
 // ---- writers ----
 
 // Formats rows [0, n) with fmt_row(i, buf) -> bytes written, in parallel chunks, and writes

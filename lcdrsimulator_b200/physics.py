@@ -111,6 +111,7 @@ def estimate_stable_dt_window(r: DtRequest) -> dict:
     if aniso:
         dt_diff_total *= 0.25
     dt_diff = dt_diff_total
+    L_ex = L_eff
     semi = False
     if r.use_semi_implicit and r.L_stab > 0.0 and r.jacobi_iters > 0:
         L_base = r.L1 if using_ldg else r.kappa
@@ -137,5 +138,6 @@ def estimate_stable_dt_window(r: DtRequest) -> dict:
     dt_max = min(dt_diff, dt_bulk)
     if not (dt_max > 0.0) or not math.isfinite(dt_max):
         dt_max = dt_diff
-    return dict(min_dx=min_dx, S_scale=S_scale, D_total=D, dt_diff_total=dt_diff_total, dt_diff=dt_diff,
-                dt_bulk=dt_bulk, dt_max=dt_max, semi_implicit_active=semi)
+    return dict(min_dx=min_dx, S_scale=S_scale, L_eff_total=L_eff, D_total=D, dt_diff_total=dt_diff_total,
+                L_eff_explicit=L_ex, dt_diff=dt_diff, bulk_rate=bulk_rate, dt_bulk=dt_bulk, dt_max=dt_max,
+                semi_implicit_active=semi)

@@ -1,0 +1,26 @@
+// Plain-pointer exports of the drop-in host programs' step scalars -- TEST INFRASTRUCTURE ONLY.
+//
+// Compiles the product's lcdrsimulator_b200/host/host_common.hpp (the restatement the qsr_b200
+// host program calls) so that tests can compare it number for number with the reference's own
+// estimate_stable_dt_window and resolve_boundary_shell_order (QSR.cu:1475-1487, 1528-1604),
+// which oracle/ref_cuda_harness.cu exports from the reference build.
+#include "host_common.hpp"
+
+extern "C" {
+
+// Same argument and output order as qref_dt_window in ref_cuda_harness.cu.
+void hshim_dt_window(const double* req, double* out) {
+    const host::DtResult e = host::estimate_dt(req[0], req[1], req[2], req[3], req[4], req[5], req[6], req[7],
+                                               (int)req[8], req[9], req[10], req[11], req[12], req[13], req[14],
+                                               req[15], req[16], req[17] != 0.0, req[18], (int)req[19]);
+    const double v[11] = {e.min_dx, e.S_scale, e.L_eff_total, e.D_total, e.dt_diff_total, e.L_eff_explicit,
+                          e.dt_diff, e.bulk_rate, e.dt_bulk, e.dt_max, e.semi_implicit_active ? 1.0 : 0.0};
+    for (int n = 0; n < 11; ++n) out[n] = v[n];
+}
+
+double hshim_shell_order(int custom, double custom_S, double a, double b, double c, double T, double T_star,
+                         int modechoice) {
+    return host::resolve_shell_order(custom != 0, custom_S, a, b, c, T, T_star, modechoice);
+}
+
+}  // extern "C"

@@ -243,15 +243,29 @@ class RefCPU:
         return out
 
     def run_steps(self, p, q, T, S_shell, dt, n_steps):
-        """n_steps of the reference CPU time step in place; returns the loop's wall seconds."""
+        """n_steps of the reference CPU time step in place (droplet mask of radius
+        p.droplet_radius_cells when positive); returns the loop's wall seconds."""
         self.L.ref_run_steps.restype = C.c_double
         return self.L.ref_run_steps(_ptr(q), p.Nx, p.Ny, p.Nz, C.c_double(p.dx), C.c_double(p.dy),
                                     C.c_double(p.dz), _ptr(self._pr(p, T)), C.c_double(p.kappa),
                                     C.c_int(p.bulk_modechoice), C.c_double(p.gamma), C.c_double(dt),
-                                    C.c_double(S_shell), C.c_int(n_steps))
+                                    C.c_double(S_shell), C.c_int(n_steps), C.c_double(p.droplet_radius_cells))
 
     def max_threads(self):
         return self.L.ref_max_threads()
+
+
+def ref_initial_field(p: OrcParams, mode, seed, S0, noise_amplitude=1e-3) -> np.ndarray:
+    """The reference's own seeded initial field: initializeQTensor / initializeIsotropicWithNoise
+    (QSR.cu:1841-1904) from the reference build (host code; no GPU needed)."""
+    path = os.path.join(REF, "qsr_cuda_ref.so")
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    L = C.CDLL(path)
+    L.qref_init.argtypes = [C.c_int] * 3 + [C.c_double] * 4 + [C.c_int, C.c_longlong, C.c_double, C.c_double, _dp]
+    q = np.zeros(p.Nx * p.Ny * p.Nz * 5)
+    L.qref_init(p.Nx, p.Ny, p.Nz, p.dx, p.dy, p.dz, p.droplet_radius_cells, mode, seed, S0, noise_amplitude, _ptr(q))
+    return q
 
 
 class RefCUDA:

@@ -237,6 +237,51 @@ int qref_observe(double T, double S_shell, int dz_slice, double dS_thr, double d
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
 }
 
+// ---- host-only wrappers of the reference's step scalars and initialisation (no GPU needed) ----
+
+// estimate_stable_dt_window (QSR.cu:1528-1604). req: dx dy dz gamma a b c T_star modechoice kappa L1 L2
+// L3 S_ref_used S0 T_a T_b use_semi_implicit L_stab jacobi_iters. out: min_dx S_scale L_eff_total
+// D_total dt_diff_total L_eff_explicit dt_diff bulk_rate dt_bulk dt_max semi_implicit_active.
+void qref_dt_window(const double* req, double* out) {
+    DtEstimateRequest r;
+    r.dx = req[0]; r.dy = req[1]; r.dz = req[2]; r.gamma = req[3];
+    r.a = req[4]; r.b = req[5]; r.c = req[6]; r.T_star = req[7]; r.modechoice = (int)req[8];
+    r.kappa = req[9]; r.L1 = req[10]; r.L2 = req[11]; r.L3 = req[12];
+    r.S_ref_used = req[13]; r.S0 = req[14]; r.T_a = req[15]; r.T_b = req[16];
+    r.use_semi_implicit = req[17] != 0.0; r.L_stab = req[18]; r.jacobi_iters = (int)req[19];
+    const DtEstimateResult e = estimate_stable_dt_window(r);
+    const double v[11] = {e.min_dx, e.S_scale, e.L_eff_total, e.D_total, e.dt_diff_total, e.L_eff_explicit,
+                          e.dt_diff, e.bulk_rate, e.dt_bulk, e.dt_max, e.semi_implicit_active ? 1.0 : 0.0};
+    std::memcpy(out, v, sizeof(v));
+}
+
+// resolve_boundary_shell_order (QSR.cu:1475-1487); custom != 0 selects BoundaryOrderMode::Custom.
+double qref_shell_order(int custom, double custom_S, double a, double b, double c, double T, double T_star,
+                        int modechoice) {
+    return resolve_boundary_shell_order(custom ? BoundaryOrderMode::Custom : BoundaryOrderMode::Equilibrium,
+                                        custom_S, a, b, c, T, T_star, modechoice);
+}
+
+// initializeQTensor (modes 0, 1) / initializeIsotropicWithNoise (mode 2) (QSR.cu:1841-1904), as main
+// dispatches them (QSR.cu:2510-2515), on the reference droplet of an Nx x Ny x Nz grid with the
+// optional radius override of qref_create. q: 5 doubles per cell, reference cell order.
+void qref_init(int Nx, int Ny, int Nz, double dx, double dy, double dz, double radius_cells, int mode,
+               long long seed, double S0, double noise_amplitude, double* q) {
+    DropletGeometry g = makeDropletGeometry(Nx, Ny, Nz, dx, dy, dz);
+    if (radius_cells > 0.0) {
+        g.radius_x = std::max(radius_cells * dx, 0.5 * dx);
+        g.radius_y = std::max(radius_cells * dy, 0.5 * dy);
+        g.radius_z = std::max(radius_cells * dz, 0.5 * dz);
+        g.min_radius = std::min({g.radius_x, g.radius_y, g.radius_z});
+    }
+    std::vector<QTensor> h;
+    if (mode == 2)
+        initializeIsotropicWithNoise(h, Nx, Ny, Nz, noise_amplitude, g, seed);
+    else
+        initializeQTensor(h, Nx, Ny, Nz, S0, mode, g, seed);
+    std::memcpy(q, h.data(), h.size() * sizeof(QTensor));
+}
+
 void qref_destroy(void) {
     cudaFree(S.Q); cudaFree(S.Qalt); cudaFree(S.lap); cudaFree(S.mu); cudaFree(S.rhs); cudaFree(S.shell);
     cudaFree(S.Dx); cudaFree(S.Dy); cudaFree(S.Dz); cudaFree(S.eb); cudaFree(S.ee); cudaFree(S.ea);

@@ -65,14 +65,16 @@ void ref_energy(const double* q, int Nx, int Ny, int Nz, double dx, double dy, d
 
 // n_steps of the reference CPU time step (QSR.cpp:395-400 chain: Laplacian, chemical
 // potential, weak anchoring, update, boundary conditions) on the reference CPU's own droplet
-// mask |r - R| < 1, R = min(N)/2, centre N/2 (QSR.cpp:1091-1101). Returns wall seconds of the
-// stepping loop only.
+// mask |r - R| < 1, centre N/2 (QSR.cpp:1091-1101), R = min(N)/2 there, or radius_cells when
+// that is positive (so that the mask matches a workload's droplet size). Returns wall seconds
+// of the stepping loop only.
 double ref_run_steps(double* q, int Nx, int Ny, int Nz, double dx, double dy, double dz, const double* params,
-                     double kappa, int modechoice, double gamma, double dt, double S_shell, int n_steps) {
+                     double kappa, int modechoice, double gamma, double dt, double S_shell, int n_steps,
+                     double radius_cells) {
     const long long n = (long long)Nx * Ny * Nz;
     std::vector<QTensor> Q = to_vec(q, n), L(n), M(n);
     std::vector<bool> is_shell(n, false);
-    const double R = std::min({(double)Nx, (double)Ny, (double)Nz}) / 2.0;
+    const double R = radius_cells > 0.0 ? radius_cells : std::min({(double)Nx, (double)Ny, (double)Nz}) / 2.0;
     const double cx = Nx / 2.0, cy = Ny / 2.0, cz = Nz / 2.0;
     for (int i = 0; i < Nx; ++i)
         for (int j = 0; j < Ny; ++j)

@@ -41,8 +41,13 @@ def test_oracle_matches_reference_cuda_fixture(oracle, path):
     ref = z["q_final"]
     assert np.abs(q1 - ref).max() <= 1e-12 * np.abs(ref).max()
     o = oracle.observe(op, g, fl, ref, T, S)
-    for k in ("bulk", "elastic", "anchoring", "radiality", "avg_S", "max_S"):
+    for k in ("bulk", "elastic", "anchoring", "radiality", "avg_S", "max_S", "defect_density"):
         assert o[k] == pytest.approx(float(z["obs_" + k]), rel=1e-12, abs=1e-300), k
+    # checker = |sum_even - sum_odd| / sum (QSR.cu:2839-2873): a cancelling difference, so its
+    # rounding error is a few ulps of the sums (absolute), not of the small ratio
+    assert o["checker_rel"] == pytest.approx(float(z["obs_checker_rel"]), rel=0, abs=1e-13), "checker_rel"
+    # the reference sums the xi proxy with FP64 atomics (QSR.cu:1042-1106): order-dependent rounding
+    assert o["xi_grad_proxy"] == pytest.approx(float(z["obs_xi_grad_proxy"]), rel=1e-12), "xi_grad_proxy"
     for k in ("defect_count", "defect_plaquettes", "xi_edges"):
         assert o[k] == int(z["obs_" + k]), k
 
