@@ -570,8 +570,9 @@ def main():
         alg_bytes += 40 * written  # low words of the changing cells read and written
     if imex:
         # IMEX step: the RHS kernel (visited cells read, moving cells' RHS written) plus one pass
-        # per Jacobi sweep, each reading the field and the RHS and writing the field
-        alg_bytes += imex["jacobi"] * 60 * box
+        # per Jacobi sweep over the changing cells: each reads and writes the field (moving and
+        # strongly anchored cells) and reads the RHS of the moving cells
+        alg_bytes += imex["jacobi"] * (40 * written + 20 * geo["evolving_cells"])
     achieved = alg_bytes / t_step / 1e9
     # the committed DRAM traffic was captured with plain FP32 storage
     traffic = None if (args.compensated or args.grid) else load_traffic(args.workload, alg_bytes)

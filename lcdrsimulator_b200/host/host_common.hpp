@@ -263,9 +263,18 @@ inline bool save_qtensor(const std::vector<double>& q, int Nx, int Ny, int Nz, c
     });
 }
 
+// The traceless/symmetric check of a warm-start file, in FP64: the largest |Qxx + Qyy + Qzz| and
+// |Q_ab - Q_ba| over the file's rows, and its largest |Q_ab|.
+struct QtensorFileCheck {
+    double max_trace = 0.0, max_asymmetry = 0.0, max_entry = 0.0;
+};
+
 // Reader of the Qtensor_output_*.dat format (warm start / resume): fills the 5 independent
-// components; returns false on a malformed file or a grid mismatch.
-inline bool load_qtensor(const std::string& path, int Nx, int Ny, int Nz, std::vector<double>& q, std::string& err) {
+// components; returns false on a malformed file or a grid mismatch. With `check`, also measures
+// how far the file's 9 entries per row are from a traceless symmetric tensor (the stored field
+// keeps Qxx, Qxy, Qxz, Qyy, Qyz; Qzz = -(Qxx + Qyy) and the symmetric entries are implied).
+inline bool load_qtensor(const std::string& path, int Nx, int Ny, int Nz, std::vector<double>& q, std::string& err,
+                         QtensorFileCheck* check = nullptr) {
     FILE* f = std::fopen(path.c_str(), "r");
     if (!f) { err = "cannot open " + path; return false; }
     const long long n = (long long)Nx * Ny * Nz;
@@ -291,6 +300,12 @@ inline bool load_qtensor(const std::string& path, int Nx, int Ny, int Nz, std::v
         const long long t = (long long)k + (long long)Nz * ((long long)j + (long long)Ny * i);
         double* c = &q[5 * t];
         c[0] = v[0]; c[1] = v[1]; c[2] = v[2]; c[3] = v[4]; c[4] = v[5];
+        if (check) {
+            check->max_trace = std::max(check->max_trace, std::abs(v[0] + v[4] + v[8]));
+            check->max_asymmetry = std::max({check->max_asymmetry, std::abs(v[1] - v[3]), std::abs(v[2] - v[6]),
+                                             std::abs(v[5] - v[7])});
+            for (double x : v) check->max_entry = std::max(check->max_entry, std::abs(x));
+        }
         seen[t] = 1;
         ++rows;
     }

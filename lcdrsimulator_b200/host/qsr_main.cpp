@@ -292,8 +292,18 @@ int run_main(int argc, char** argv) {
         const std::string init_file = get_string(cfg, "init_file", "");
         if (!init_file.empty()) {
             std::string err;
-            if (!load_qtensor(init_file, Nx, Ny, Nz, h_Q, err)) throw Fail{"init_file: " + err};
-            std::cout << "[Init] Warm start from " << init_file << std::endl;
+            QtensorFileCheck chk{};
+            if (!load_qtensor(init_file, Nx, Ny, Nz, h_Q, err, &chk)) throw Fail{"init_file: " + err};
+            std::cout << "[Init] Warm start from " << init_file << " (max |tr Q| = " << chk.max_trace
+                      << ", max |Q - Q^T| = " << chk.max_asymmetry << ", max |Q| = " << chk.max_entry << ")"
+                      << std::endl;
+            // the stored field is traceless and symmetric by construction (five independent
+            // components); a file further from that than its own %.6e rounding is not a Q tensor
+            const double tol = 1e-5 * chk.max_entry;
+            if (chk.max_trace > tol || chk.max_asymmetry > tol)
+                throw Fail{"init_file: not a traceless symmetric tensor field (max |tr Q| = " +
+                           std::to_string(chk.max_trace) + ", max |Q - Q^T| = " + std::to_string(chk.max_asymmetry) +
+                           ")"};
         } else if (mode == 2) {
             const double amp = get<double>(cfg, "noise_amplitude", noise_default);
             check(qsr_initial_field(R.h, 2, random_seed, S0, amp, h_Q.data()), "qsr_initial_field");

@@ -6,6 +6,10 @@
 // which oracle/ref_cuda_harness.cu exports from the reference build.
 #include "host_common.hpp"
 
+#include <algorithm>
+#include <string>
+#include <vector>
+
 extern "C" {
 
 // Same argument and output order as qref_dt_window in ref_cuda_harness.cu.
@@ -21,6 +25,28 @@ void hshim_dt_window(const double* req, double* out) {
 double hshim_shell_order(int custom, double custom_S, double a, double b, double c, double T, double T_star,
                          int modechoice) {
     return host::resolve_shell_order(custom != 0, custom_S, a, b, c, T, T_star, modechoice);
+}
+
+// The host programs' writers (host_common.hpp) and the warm-start reader, on a caller's field.
+int hshim_save_qtensor(const double* q, int Nx, int Ny, int Nz, const char* path) {
+    const std::vector<double> v(q, q + 5 * (size_t)Nx * Ny * Nz);
+    return host::save_qtensor(v, Nx, Ny, Nz, path) ? 0 : 1;
+}
+
+int hshim_save_nematic(const double* s_n4, int Nx, int Ny, int Nz, const char* path) {
+    const std::vector<double> v(s_n4, s_n4 + 4 * (size_t)Nx * Ny * Nz);
+    return host::save_nematic(v, Nx, Ny, Nz, path) ? 0 : 1;
+}
+
+// out3: the file's largest |trace| and |asymmetry| and the largest |Q| entry.
+int hshim_load_qtensor(const char* path, int Nx, int Ny, int Nz, double* q, double* out3) {
+    std::vector<double> v;
+    std::string err;
+    host::QtensorFileCheck chk{};
+    if (!host::load_qtensor(path, Nx, Ny, Nz, v, err, &chk)) return 1;
+    std::copy(v.begin(), v.end(), q);
+    out3[0] = chk.max_trace; out3[1] = chk.max_asymmetry; out3[2] = chk.max_entry;
+    return 0;
 }
 
 }  // extern "C"

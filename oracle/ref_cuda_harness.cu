@@ -282,6 +282,22 @@ void qref_init(int Nx, int Ny, int Nz, double dx, double dy, double dz, double r
     std::memcpy(q, h.data(), h.size() * sizeof(QTensor));
 }
 
+// The reference's text writers on a caller's field: saveQTensorToFile (QSR.cu:1818-1832) from 5
+// doubles per cell, saveNematicFieldToFile (QSR.cu:1802-1816) from (S, nx, ny, nz) per cell.
+void qref_save_qtensor(const double* q, int Nx, int Ny, int Nz, const char* path) {
+    std::vector<QTensor> h((size_t)Nx * Ny * Nz);
+    std::memcpy(h.data(), q, h.size() * sizeof(QTensor));
+    saveQTensorToFile(h, Nx, Ny, Nz, path);
+}
+
+void qref_save_nematic(const double* s_n4, int Nx, int Ny, int Nz, const char* path) {
+    std::vector<NematicField> h((size_t)Nx * Ny * Nz);
+    for (size_t t = 0; t < h.size(); ++t) {
+        h[t].S = s_n4[4 * t]; h[t].nx = s_n4[4 * t + 1]; h[t].ny = s_n4[4 * t + 2]; h[t].nz = s_n4[4 * t + 3];
+    }
+    saveNematicFieldToFile(h, Nx, Ny, Nz, path);
+}
+
 void qref_destroy(void) {
     cudaFree(S.Q); cudaFree(S.Qalt); cudaFree(S.lap); cudaFree(S.mu); cudaFree(S.rhs); cudaFree(S.shell);
     cudaFree(S.Dx); cudaFree(S.Dy); cudaFree(S.Dz); cudaFree(S.eb); cudaFree(S.ee); cudaFree(S.ea);
