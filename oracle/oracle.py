@@ -352,6 +352,17 @@ class RefKZM:
         assert rc == 0, rc
         return ms.value
 
+    def quench(self, bp, q, seed, a, b, c, T_star, T_high, T_low, pre, ramp, total, noise_strength, mode=1):
+        """The reference's quench loop (KZM_bulk_ldg.cu:917-970) over total iterations; returns the
+        final field and the (A, B, C) of the final temperature."""
+        out = np.zeros_like(q)
+        r = np.array([a, b, c, T_star, mode, T_high, T_low, pre, ramp, total, noise_strength], dtype=np.float64)
+        abc = np.zeros(3)
+        rc = self.L.kref_quench(_ptr(self._arr(bp)), _ptr(r), _ptr(np.ascontiguousarray(q)), _ptr(out),
+                                C.c_ulonglong(seed), _ptr(abc))
+        assert rc == 0
+        return out, tuple(abc)
+
     def observe(self, bp, q, A, B, Cc):
         out = np.zeros(10)
         self.L.kref_observe(_ptr(self._arr(bp)), _ptr(np.ascontiguousarray(q)), C.c_double(A), C.c_double(B),

@@ -72,6 +72,42 @@ int kref_time(const double* p, const double* q_in, int n_warm, int n_steps, doub
     return ok ? 0 : 2;
 }
 
+// The reference's quench loop (KZM_bulk_ldg.cu:917-970) from iteration 0 to total_iters:
+// temperature compute_temperature(iter) (pre_equil_iters at T_high, linear ramp over ramp_iters,
+// then T_low), bulk coefficients bulk_ABC_from_convention, noise_sigma from noise_strength, one
+// updateBulkLdgKernel per iteration with the run's seed. r: a b c T_star modechoice T_high
+// T_low pre_equil_iters ramp_iters total_iters noise_strength. Returns the final field and
+// the (A, B, C) of the last iteration in abc_out.
+int kref_quench(const double* p, const double* r, const double* q_in, double* q_out, unsigned long long seed,
+                double* abc_out) {
+    BulkLdgParams b = make(p);
+    b.a = r[0]; b.b = r[1]; b.c = r[2]; b.T_star = r[3]; b.bulk_modechoice = (int)r[4];
+    b.T_high = r[5]; b.T_low = r[6]; b.pre_equil_iters = (int)r[7]; b.ramp_iters = (int)r[8];
+    b.total_iters = (int)r[9]; b.noise_strength = r[10];
+    const size_t n = (size_t)b.Nx * b.Ny * b.Nz;
+    QTensor *cur = nullptr, *nxt = nullptr;
+    if (cudaMalloc(&cur, n * sizeof(QTensor)) != cudaSuccess) return 1;
+    if (cudaMalloc(&nxt, n * sizeof(QTensor)) != cudaSuccess) { cudaFree(cur); return 1; }
+    cudaMemcpy(cur, q_in, n * sizeof(QTensor), cudaMemcpyHostToDevice);
+    const int bs = 256;
+    const int gs = (int)((n + bs - 1) / bs);
+    const double noise_sigma = (b.noise_strength > 0.0) ? std::sqrt(2.0 * (1.0 / b.gamma) * b.noise_strength * b.dt)
+                                                        : 0.0;
+    double A = 0.0, B = 0.0, C = 0.0;
+    for (int iter = 0; iter <= b.total_iters; ++iter) {
+        const double T = compute_temperature(b, iter);
+        bulk_ABC_from_convention(b.a, b.b, b.c, T, b.T_star, b.bulk_modechoice, A, B, C);
+        if (iter == b.total_iters) break;
+        updateBulkLdgKernel<<<gs, bs>>>(cur, nxt, b, A, B, C, noise_sigma, seed, iter);
+        std::swap(cur, nxt);
+    }
+    abc_out[0] = A; abc_out[1] = B; abc_out[2] = C;
+    cudaError_t e = cudaMemcpy(q_out, cur, n * sizeof(QTensor), cudaMemcpyDeviceToHost);
+    cudaFree(cur);
+    cudaFree(nxt);
+    return e == cudaSuccess ? 0 : 1;
+}
+
 // out: bulk elastic total avg_S max_S defect_density line_density xi plaquettes_used defects
 void kref_observe(const double* p, const double* q, double A, double B, double C, double* out) {
     const BulkLdgParams b = make(p);
