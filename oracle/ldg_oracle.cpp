@@ -936,13 +936,14 @@ extern "C" void orc_bulk_observe(const orc_bulk_params* p, const double* q, doub
 }
 
 // ---------------------------------------------------------------------------------------
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
-// SC'11): 10 rounds of two 32x32->64 multiplies with the published constants.
+// Philox4x32-R (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): R rounds of two 32x32->64 multiplies with the published constants (R = 10 is the
+// paper's default and has published known answers; the device noise uses R = 7).
 // ---------------------------------------------------------------------------------------
-extern "C" void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+extern "C" void orc_philox4x32_rounds(const uint32_t ctr[4], const uint32_t key[2], int rounds, uint32_t out[4]) {
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
     uint32_t k0 = key[0], k1 = key[1];
-    for (int r = 0; r < 10; ++r) {
+    for (int r = 0; r < rounds; ++r) {
         const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
         const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
         const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
@@ -953,4 +954,8 @@ extern "C" void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uin
         k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
     }
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+extern "C" void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    orc_philox4x32_rounds(ctr, key, 10, out);
 }

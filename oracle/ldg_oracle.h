@@ -110,8 +110,9 @@ void orc_bulk_step(const orc_bulk_params* p, const double* q, double* q_next,
 void orc_bulk_observe(const orc_bulk_params* p, const double* q, double A, double B, double C,
                       orc_bulk_observables* out);
 
-/* ---- Philox4x32-10 counter-based generator (Salmon et al., SC'11) ---- */
+/* ---- Philox4x32-R counter-based generator (Salmon et al., SC'11): R = 10 (known answers), R = 7 (device noise) ---- */
 void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void orc_philox4x32_rounds(const uint32_t ctr[4], const uint32_t key[2], int rounds, uint32_t out[4]);
 
 #ifdef __cplusplus
 }

@@ -196,11 +196,11 @@ class Oracle:
         self.L.orc_bulk_observe(C.byref(bp), _ptr(q), C.c_double(A), C.c_double(B), C.c_double(Cc), C.byref(o))
         return o.as_dict()
 
-    def philox(self, ctr, key):
+    def philox(self, ctr, key, rounds=10):
         c = (C.c_uint32 * 4)(*ctr)
         k = (C.c_uint32 * 2)(*key)
         o = (C.c_uint32 * 4)()
-        self.L.orc_philox4x32(c, k, o)
+        self.L.orc_philox4x32_rounds(c, k, C.c_int(rounds), o)
         return list(o)
 
 

@@ -11,7 +11,7 @@ five ramps tau_Q = 500 .. 8000 steps, each followed by a 2000-step hold at 295 K
 seeds per rate.
 
 Both sides start from the reference's own initial field (mt19937_64 Gaussian, seed per run) and
-follow the reference's temperature schedule; the noise streams differ (Philox4x32-10 here,
+follow the reference's temperature schedule; the noise streams differ (Philox4x32-7 here,
 splitmix64 in the reference), so single runs differ and the comparison is statistical: the mean
 final line density at every rate within 4 combined standard errors, and the two fitted slopes
 within 3 combined standard deviations (seed bootstrap). The measured slopes and their spread are

@@ -144,7 +144,9 @@ def test_long_run_fp32_error_budget(oracle):
 @pytest.mark.parametrize("grid", [dict(Nx=8, Ny=8, Nz=8), dict(Nx=12, Ny=20, Nz=72, droplet_radius_cells=9.0)])
 def test_noise_stream_matches_philox_box_muller(oracle, grid):
     # With Q = 0, A = 0 (T = T*) and no gradients the update is the noise alone, so the device
-    # noise can be read back and compared with Philox4x32-10 + Box-Muller evaluated here.
+    # noise can be read back and compared with Philox4x32-7 + Box-Muller evaluated here. The
+    # device radius uses the hardware base-2 logarithm (absolute error <= 2^-22 near u = 1), so a
+    # normal may be off by 2e-4 in absolute terms where |z| is tiny, 1e-5 relative elsewhere.
     # The second grid has tiles on the face-free interior path.
     op, solver, d = make_pair(L1=6e-12, W=1e-5, **grid)
     g, fl = oracle.geometry(op)
@@ -157,7 +159,7 @@ def test_noise_stream_matches_philox_box_muller(oracle, grid):
     idx = np.flatnonzero(move)
     m21 = (1 << 21) - 1
     for cell in idx[:: max(1, len(idx) // 40)]:
-        w = oracle.philox([int(cell), 0, step & 0xFFFFFFFF, step >> 32], [k0, k1])
+        w = oracle.philox([int(cell), 0, step & 0xFFFFFFFF, step >> 32], [k0, k1], rounds=7)
         f = [w[0] & m21, w[1] & m21, w[2] & m21, w[3] & m21, ((w[0] >> 21) << 10) | (w[1] >> 22),
              ((w[2] >> 21) << 10) | (w[3] >> 22)]
         u = [(x + 1.0) / 2097152.0 for x in f]
@@ -165,7 +167,7 @@ def test_noise_stream_matches_philox_box_muller(oracle, grid):
         z = [r[0] * math.cos(2 * math.pi * u[1]), r[0] * math.sin(2 * math.pi * u[1]),
              r[1] * math.cos(2 * math.pi * u[3]), r[1] * math.sin(2 * math.pi * u[3]),
              r[2] * math.cos(2 * math.pi * u[5])]
-        assert np.allclose(got[cell], sigma * np.array(z), rtol=2e-5, atol=1e-5 * sigma)
+        assert np.allclose(got[cell], sigma * np.array(z), rtol=2e-5, atol=2e-4 * sigma)
     assert np.all(got[~move] == 0.0)
     # distribution: zero mean, unit variance over all evolving cells and components
     zs = got[move].ravel() / sigma

@@ -2,7 +2,7 @@
 
 The reference's periodic bulk kernel (KZM_bulk_ldg.cu, built from its sources into oracle/_ref
 and run on the GPU in FP64) draws its Langevin noise from a splitmix64 stream; this library
-draws it from Philox4x32-10. Single trajectories therefore differ, but their statistics over
+draws it from Philox4x32-7. Single trajectories therefore differ, but their statistics over
 seeds must agree. A 32^3 periodic box is quenched to 300 K from the same 12 isotropic initial
 fields (|Q| ~ 1e-3) with noise kT/dx^3 at 300 K; at four times the means over seeds of the
 average order S, the free energy and the defect line density must agree within 4 combined
