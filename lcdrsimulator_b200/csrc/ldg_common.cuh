@@ -330,6 +330,141 @@ __device__ __forceinline__ void chem_potential(const Acc& A, const DAcc& DA, con
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Packed-pair form of the interior chemical potential. Blackwell issues one FFMA2 / FADD2 /
+// FMUL2 for two FP32 lanes, so the stencil arithmetic runs on component pairs: X = (xx, yy),
+// Y = (xy, xz); yz stays scalar and zz = -(xx + yy). Same terms and weights as
+// chem_potential<kL2, kL3, false>; only the rounding order differs.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b as b * (-1) + a (the product is exact, so this is the rounded difference)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+
+template <bool kL2, bool kL3, class Acc, class DAcc>
+__device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const DAcc& DA, const QsrConst& P, int i,
+                                                           int j, int k, const float q[5], bool anchor, float mu[5],
+                                                           float lap[5]) {
+    auto X = [&](int di, int dj, int dk) { return make_float2(A(0, di, dj, dk), A(3, di, dj, dk)); };
+    auto Y = [&](int di, int dj, int dk) { return make_float2(A(1, di, dj, dk), A(2, di, dj, dk)); };
+    auto Z = [&](int di, int dj, int dk) { return A(4, di, dj, dk); };  // yz
+    const float2 qX = make_float2(q[0], q[3]), qY = make_float2(q[1], q[2]);
+    const float qZ = q[4];
+    // face neighbours, their sums (Laplacian, pure second derivatives) and undivided central
+    // differences (first derivatives)
+    const float2 Xpx = X(1, 0, 0), Xmx = X(-1, 0, 0), Xpy = X(0, 1, 0), Xmy = X(0, -1, 0), Xpz = X(0, 0, 1),
+                 Xmz = X(0, 0, -1);
+    const float2 Ypx = Y(1, 0, 0), Ymx = Y(-1, 0, 0), Ypy = Y(0, 1, 0), Ymy = Y(0, -1, 0), Ypz = Y(0, 0, 1),
+                 Ymz = Y(0, 0, -1);
+    const float Zpx = Z(1, 0, 0), Zmx = Z(-1, 0, 0), Zpy = Z(0, 1, 0), Zmy = Z(0, -1, 0), Zpz = Z(0, 0, 1),
+                Zmz = Z(0, 0, -1);
+    const float2 sxX = add2(Xpx, Xmx), syX = add2(Xpy, Xmy), szX = add2(Xpz, Xmz);
+    const float2 sxY = add2(Ypx, Ymx), syY = add2(Ypy, Ymy), szY = add2(Ypz, Ymz);
+    const float sxZ = Zpx + Zmx, syZ = Zpy + Zmy, szZ = Zpz + Zmz;
+    const float2 lapX = fma2(bc2(P.ix2), sxX, fma2(bc2(P.iy2), syX, fma2(bc2(P.iz2), szX, mul2(bc2(P.lap_c), qX))));
+    const float2 lapY = fma2(bc2(P.ix2), sxY, fma2(bc2(P.iy2), syY, fma2(bc2(P.iz2), szY, mul2(bc2(P.lap_c), qY))));
+    const float lapZ = fmaf(P.ix2, sxZ, fmaf(P.iy2, syZ, fmaf(P.iz2, szZ, P.lap_c * qZ)));
+    lap[0] = lapX.x; lap[3] = lapX.y; lap[1] = lapY.x; lap[2] = lapY.y; lap[4] = lapZ;
+    float h[6];
+    bulk_field(q, P.cQ, P.cQ2, P.cQ3, h);
+    // elastic (one-constant or L1): hX = (h_xx, h_yy), hY = (h_xy, h_xz), h_zz, h_yz
+    float2 hX = fma2(bc2(-P.Liso), lapX, make_float2(h[0], h[1]));
+    float2 hY = fma2(bc2(-P.Liso), lapY, make_float2(h[3], h[4]));
+    float hzz = fmaf(P.Liso, lapX.x + lapX.y, h[2]);  // - Liso lap_zz, lap_zz = -(lap_xx + lap_yy)
+    float hyz = fmaf(-P.Liso, lapZ, h[5]);
+    if (kL2) {
+        // h -= L2 d_a D_b (central differences of the staged column divergence, QSR.cu:436-460)
+        hX = fma2(make_float2(-P.L2i2x, -P.L2i2y),
+                  sub2(make_float2(DA(0, 1, 0, 0), DA(1, 0, 1, 0)), make_float2(DA(0, -1, 0, 0), DA(1, 0, -1, 0))), hX);
+        hY = fma2(bc2(-P.L2i2x),
+                  sub2(make_float2(DA(1, 1, 0, 0), DA(2, 1, 0, 0)), make_float2(DA(1, -1, 0, 0), DA(2, -1, 0, 0))), hY);
+        hY = fma2(make_float2(-P.L2i2y, -P.L2i2z),
+                  sub2(make_float2(DA(0, 0, 1, 0), DA(0, 0, 0, 1)), make_float2(DA(0, 0, -1, 0), DA(0, 0, 0, -1))), hY);
+        hzz = fmaf(-P.L2i2z, DA(2, 0, 0, 1) - DA(2, 0, 0, -1), hzz);
+        hyz = fmaf(-P.L2i2y, DA(2, 0, 1, 0) - DA(2, 0, -1, 0), hyz);
+        hyz = fmaf(-P.L2i2z, DA(1, 0, 0, 1) - DA(1, 0, 0, -1), hyz);
+    }
+    float corr = (hX.x + hX.y + hzz) * (1.0f / 3.0f);
+    float2 muX = add2(hX, bc2(-corr));  // (mu_xx, mu_yy)
+    float2 muY = hY;                    // (mu_xy, mu_xz)
+    float muZ = hyz;                    // mu_yz
+    if (kL3) {
+        // undivided central differences per axis
+        const float2 dXx = sub2(Xpx, Xmx), dXy = sub2(Xpy, Xmy), dXz = sub2(Xpz, Xmz);
+        const float2 dYx = sub2(Ypx, Ymx), dYy = sub2(Ypy, Ymy), dYz = sub2(Ypz, Ymz);
+        const float dZx = Zpx - Zmx, dZy = Zpy - Zmy, dZz = Zpz - Zmz;
+        const float d5x = -(dXx.x + dXx.y), d5y = -(dXy.x + dXy.y), d5z = -(dXz.x + dXz.y);  // zz
+        // M_ab = dQ_kl/da dQ_kl/db over all nine entries: xx, yy, zz once, off-diagonals twice
+        const float2 dYx2 = add2(dYx, dYx), dYy2 = add2(dYy, dYy), dYz2 = add2(dYz, dYz);
+        auto M = [&](float2 xa, float2 xb, float2 ya, float2 yb2, float za, float zb, float va, float vb) {
+            const float2 t = fma2(ya, yb2, mul2(xa, xb));
+            return fmaf(2.0f * za, zb, fmaf(va, vb, t.x + t.y));
+        };
+        float hxx = fmaf(P.l3m[0], M(dXx, dXx, dYx, dYx2, dZx, dZx, d5x, d5x), muX.x);
+        float hyy = fmaf(P.l3m[1], M(dXy, dXy, dYy, dYy2, dZy, dZy, d5y, d5y), muX.y);
+        float hz = fmaf(P.l3m[2], M(dXz, dXz, dYz, dYz2, dZz, dZz, d5z, d5z), -(muX.x + muX.y));
+        float hxy = fmaf(P.l3m[3], M(dXx, dXy, dYx, dYy2, dZx, dZy, d5x, d5y), muY.x);
+        float hxz = fmaf(P.l3m[4], M(dXx, dXz, dYx, dYz2, dZx, dZz, d5x, d5z), muY.y);
+        float hyz3 = fmaf(P.l3m[5], M(dXy, dXz, dYy, dYz2, dZy, dZz, d5y, d5z), muZ);
+        // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603) on all components at once:
+        // weights of the six second derivatives, shared by every component
+        const float Qzz = -q[0] - q[3];
+        const float2 wxx = bc2(q[0] * P.ix2), wyy = bc2(q[3] * P.iy2), wzz = bc2(Qzz * P.iz2);
+        const float2 wxy = bc2(2.0f * q[1] * P.i4xy), wxz = bc2(2.0f * q[2] * P.i4xz), wyz = bc2(2.0f * q[4] * P.i4yz);
+        const float2 Dc0 = bc2(DA(0, 0, 0, 0) * P.i2x), Dc1 = bc2(DA(1, 0, 0, 0) * P.i2y),
+                     Dc2 = bc2(DA(2, 0, 0, 0) * P.i2z);
+        auto mixedX = [&](int a, int b) {
+            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
+            pa[a] = 1; pb[b] = 1;
+            return sub2(sub2(X(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]), X(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])),
+                        sub2(X(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]),
+                             X(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2])));
+        };
+        auto mixedY = [&](int a, int b) {
+            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
+            pa[a] = 1; pb[b] = 1;
+            return sub2(sub2(Y(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]), Y(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])),
+                        sub2(Y(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]),
+                             Y(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2])));
+        };
+        auto mixedZ = [&](int a, int b) {
+            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
+            pa[a] = 1; pb[b] = 1;
+            return (Z(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]) - Z(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])) -
+                   (Z(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]) - Z(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2]));
+        };
+        const float2 q2X = add2(qX, qX), q2Y = add2(qY, qY);
+        const float2 cX = fma2(wxx, sub2(sxX, q2X), fma2(wyy, sub2(syX, q2X), fma2(wzz, sub2(szX, q2X),
+                          fma2(wxy, mixedX(0, 1), fma2(wxz, mixedX(0, 2), mul2(wyz, mixedX(1, 2)))))));
+        const float2 cY = fma2(wxx, sub2(sxY, q2Y), fma2(wyy, sub2(syY, q2Y), fma2(wzz, sub2(szY, q2Y),
+                          fma2(wxy, mixedY(0, 1), fma2(wxz, mixedY(0, 2), mul2(wyz, mixedY(1, 2)))))));
+        const float q2Z = 2.0f * qZ;
+        const float cZ = fmaf(wxx.x, sxZ - q2Z, fmaf(wyy.x, syZ - q2Z, fmaf(wzz.x, szZ - q2Z,
+                         fmaf(wxy.x, mixedZ(0, 1), fmaf(wxz.x, mixedZ(0, 2), wyz.x * mixedZ(1, 2))))));
+        const float2 BX = fma2(Dc0, dXx, fma2(Dc1, dXy, fma2(Dc2, dXz, cX)));  // (B_xx, B_yy)
+        const float2 BY = fma2(Dc0, dYx, fma2(Dc1, dYy, fma2(Dc2, dYz, cY)));  // (B_xy, B_xz)
+        const float BZ = fmaf(Dc0.x, dZx, fmaf(Dc1.x, dZy, fmaf(Dc2.x, dZz, cZ)));  // B_yz
+        // h -= L3 B, B_zz = -(B_xx + B_yy); re-projected traceless (QSR.cu:611-619)
+        const float2 hdX = fma2(bc2(-P.L3), BX, make_float2(hxx, hyy));
+        const float2 hdY = fma2(bc2(-P.L3), BY, make_float2(hxy, hxz));
+        hz = fmaf(P.L3, BX.x + BX.y, hz);
+        hyz3 = fmaf(-P.L3, BZ, hyz3);
+        corr = (hdX.x + hdX.y + hz) * (1.0f / 3.0f);
+        muX = add2(hdX, bc2(-corr));
+        muY = hdY;
+        muZ = hyz3;
+    }
+    mu[0] = muX.x; mu[3] = muX.y; mu[1] = muY.x; mu[2] = muY.y; mu[4] = muZ;
+    if (anchor) {
+        float Q0[5];
+        surface_q0(P, i, j, k, Q0);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) mu[c] += P.Weff * (q[c] - Q0[c]);
+    }
+}
+
 // Explicit update with compensated storage: a cell holds hi + lo (two FP32 words). The
 // increment -(dt/gamma) mu (+ noise) is added to hi exactly (Knuth's TwoSum) and the rounding
 // error carried in lo, so the stored value keeps about 48 significant bits over any number of

@@ -170,40 +170,38 @@ __global__ void __launch_bounds__(256) k_jacobi(const float* __restrict__ rhs, c
 // strongly anchored cells, each over its plane range), writing only moving and strongly anchored
 // cells. Every other cell never changes: it holds the same value in both ping-pong buffers, so
 // the reference's copy of it (QSR.cu:803-810) is already done. Block (32, 8) = one tile row per
-// warp; one work item (j0, k0, i_begin, i_end) per block.
+// warp; grid (work items, planes per item): block (x, y) sweeps plane i_begin + y of item x, so
+// every cell is an independent thread as in the full-box sweep.
 static_assert(tiled::TK == 32 && tiled::TJ == 8, "k_jacobi_tiled maps one (8 x 32) tile onto a 256-thread block");
 template <bool kLast>
 __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ rhs, const float* __restrict__ qo,
                                                       float* __restrict__ qn, const uint8_t* __restrict__ flags,
                                                       const int4* __restrict__ items, QsrConst P) {
     const int4 item = items[blockIdx.x];
+    const int i = item.z + (int)blockIdx.y;
     const int k = item.y + (int)(threadIdx.x & 31);
     const int j = item.x + (int)(threadIdx.x >> 5);
-    if (k >= P.Nz || j >= P.Ny) return;
-    const bool jk_face = (j == 0 || k == 0 || j == P.Ny - 1 || k == P.Nz - 1);
-    const long long cell0 = (long long)j * P.sj + k;
-    for (int i = item.z; i < item.w; ++i) {
-        const long long id = (long long)i * P.si + cell0;
-        const uint8_t f = __ldg(flags + id);
-        if (!(f & (kMove | kFixed))) continue;
-        float o[5];
-        if (kLast && (f & kFixed)) {
-            surface_q0(P, i, j, k, o);
-        } else if (jk_face || i == 0 || i == P.Nx - 1 || !(f & kMove)) {
+    if (i >= item.w || k >= P.Nz || j >= P.Ny) return;
+    const long long id = (long long)i * P.si + (long long)j * P.sj + k;
+    const uint8_t f = __ldg(flags + id);
+    if (!(f & (kMove | kFixed))) return;
+    float o[5];
+    if (kLast && (f & kFixed)) {
+        surface_q0(P, i, j, k, o);
+    } else if (j == 0 || k == 0 || j == P.Ny - 1 || k == P.Nz - 1 || i == 0 || i == P.Nx - 1 || !(f & kMove)) {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) o[m] = __ldg(qo + m * P.sc + id);
-        } else {
+        for (int m = 0; m < 5; ++m) o[m] = __ldg(qo + m * P.sc + id);
+    } else {
 #pragma unroll
-            for (int m = 0; m < 5; ++m) {
-                const float* b = qo + m * P.sc + id;
-                const float s = P.ix2 * (__ldg(b + P.si) + __ldg(b - P.si)) +
-                                P.iy2 * (__ldg(b + P.sj) + __ldg(b - P.sj)) + P.iz2 * (__ldg(b + 1) + __ldg(b - 1));
-                o[m] = (__ldg(rhs + m * P.sc + id) + P.alpha * s) * P.jdenom_inv;
-            }
+        for (int m = 0; m < 5; ++m) {
+            const float* b = qo + m * P.sc + id;
+            const float s = P.ix2 * (__ldg(b + P.si) + __ldg(b - P.si)) +
+                            P.iy2 * (__ldg(b + P.sj) + __ldg(b - P.sj)) + P.iz2 * (__ldg(b + 1) + __ldg(b - 1));
+            o[m] = (__ldg(rhs + m * P.sc + id) + P.alpha * s) * P.jdenom_inv;
         }
-#pragma unroll
-        for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
     }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
 }
 
 // Host AoS FP64 (reference cell order) <-> device FP32 SoA.
@@ -1094,12 +1092,12 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
                 const bool last = (it == a->jacobi_iters - 1);
                 if (tiled) {
                     if (h->tiled.n_items > 0) {
-                        const int nb = h->tiled.n_items;
+                        const dim3 jg((unsigned)h->tiled.n_items, (unsigned)h->tiled.chunk, 1);
                         if (last)
-                            k_jacobi_tiled<true><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                            k_jacobi_tiled<true><<<jg, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
                                                                             h->tiled.items, P);
                         else
-                            k_jacobi_tiled<false><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                            k_jacobi_tiled<false><<<jg, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
                                                                              h->tiled.items, P);
                     }
                 } else if (last) {

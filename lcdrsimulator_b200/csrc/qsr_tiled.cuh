@@ -40,7 +40,10 @@ constexpr int RW = TK + 2 * HK;      // 40 floats per smem row
 constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
 constexpr int CSTR = RW * ROWS;      // floats per component plane
 constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
-constexpr int NQ = 8;                // Q ring slots: planes i-2 .. i+3 in use, the rest in flight
+// Q ring slots: planes i-2 .. i+3 in use at plane i, plane i+4 in flight (issued at the end of
+// plane i). Six slots keep a CTA at ~74 KB of shared memory with the divergence ring, so three
+// CTAs (24 warps) fit on an SM, with the registers capped by the launch bounds below.
+constexpr int NQ = 6;
 constexpr int DRW = TK + 2, DROWS = TJ + 2;
 constexpr int DCSTR = DRW * DROWS;
 constexpr int DPLANE = 3 * DCSTR;
@@ -158,7 +161,8 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 
     // Plane p (p >= base) lives in slot (p - base) % NQ and completes that slot's barrier phase
     // number (p - base) / NQ of this item.
-    // (every caller has p >= base, so the ring arithmetic is unsigned: a mask and a shift)
+    // (every caller has p >= base, so the ring arithmetic is unsigned; a few times per plane)
+    static_assert(NQ >= 6, "planes i-2 .. i+3 are read at plane i");
     auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
     auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
 
@@ -289,7 +293,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                     DA.off = (jl + 1) * DRW + (kl + 1);
                     float mu[5], lap[5];
                     if (warp_interior)
-                        chem_potential<kL2, kL3, false>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                        chem_potential_interior_x2<kL2, kL3>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
                     else
                         chem_potential<kL2, kL3, true>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
                     const uint32_t cell = (uint32_t)(k + P.Nz * (j + P.Ny * i));
@@ -360,9 +364,9 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     __syncthreads();
 }
 
-// Single grid: one work item per CTA.
+// Single grid: one work item per CTA; three CTAs per SM (the bounds cap registers at 80).
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 3)
     k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
                  const int4* __restrict__ items, QsrConst P, int* __restrict__ err, const float* __restrict__ lo_in,
                  float* __restrict__ lo_out) {
@@ -433,7 +437,7 @@ __host__ __device__ __forceinline__ double ens_S_eq(double A, double B, double C
 }
 
 template <bool kL2, bool kL3, bool kNoise>
-__global__ void __launch_bounds__(THREADS, 2)
+__global__ void __launch_bounds__(THREADS, 3)
     k_step_ensemble(const CUtensorMap* __restrict__ tms, const EnsInstDev* __restrict__ inst,
                     const EnsItem* __restrict__ items, int n_items, EnsCtl* __restrict__ ctl, int* __restrict__ err) {
     constexpr bool kD = kL2 || kL3;
@@ -488,6 +492,7 @@ struct TiledPlan {
     long long active_cells = 0;   // cells inside visited tiles (each read once per step)
     long long written_cells = 0;  // cells written per step (moving + strongly anchored)
     int n_items = 0;
+    int chunk = 0;                // planes per work item (the longest item)
     int4* items = nullptr;        // device work list (j0, k0, i_begin, i_end)
     std::vector<int4> cols;       // host: per active tile column (j0, k0, i_min, i_max + 1)
     int* err = nullptr;           // device error word
@@ -548,6 +553,7 @@ inline int tiled_plan_rechunk(TiledPlan& plan, int chunk) {
     if (plan.items) cudaFree(plan.items);
     plan.items = nullptr;
     plan.n_items = (int)items.size();
+    plan.chunk = chunk;
     if (plan.n_items > 0) {
         LDG_CUDA(cudaMalloc(&plan.items, items.size() * sizeof(int4)));
         LDG_CUDA(cudaMemcpy(plan.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));

