@@ -51,6 +51,7 @@ struct QsrConst {
     float lap_c;                // -2 (1/dx^2 + 1/dy^2 + 1/dz^2): centre weight of the Laplacian
     float L2i2x, L2i2y, L2i2z;  // L2/(2d)
     float l3m[6];               // (L3/2) / (4 da db) for M_ab from undivided central differences (xx yy zz xy xz yz)
+    float l2w[6];               // L2 / (4 da db) for d_a D_b from undivided second differences (xx yy zz xy xz yz)
 };
 
 // ---------------------------------------------------------------------------------------
@@ -343,10 +344,18 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 // a - b as b * (-1) + a (the product is exact, so this is the rounded difference)
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 
-template <bool kL2, bool kL3, class Acc, class DAcc>
-__device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const DAcc& DA, const QsrConst& P, int i,
-                                                           int j, int k, const float q[5], bool anchor, float mu[5],
-                                                           float lap[5]) {
+// Interior cells (2 <= i, j, k <= N - 3 when L2 is on, else 1 <= .. <= N - 2) read only Q:
+//  * the column divergence D_b = d_k Q_kb at the centre (the L3 term's D . grad) from the face
+//    neighbours' central differences, as the reference's interior D;
+//  * the L2 term d_a D_b (QSR.cu:436-460), the central difference of the reference's central D,
+//    which for an interior cell is exactly sum_k S_ak(Q_kb) / (4 da dk): S_ak the undivided
+//    mixed (four-corner) second difference for k != a and the wide second difference
+//    Q(+2a) - 2 Q + Q(-2a) for k = a. The corner sums are the ones the L3 term needs anyway, so
+//    no divergence field is staged.
+template <bool kL2, bool kL3, class Acc>
+__device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const QsrConst& P, int i, int j, int k,
+                                                           const float q[5], bool anchor, float mu[5], float lap[5]) {
+    constexpr bool kMixed = kL2 || kL3;
     auto X = [&](int di, int dj, int dk) { return make_float2(A(0, di, dj, dk), A(3, di, dj, dk)); };
     auto Y = [&](int di, int dj, int dk) { return make_float2(A(1, di, dj, dk), A(2, di, dj, dk)); };
     auto Z = [&](int di, int dj, int dk) { return A(4, di, dj, dk); };  // yz
@@ -374,17 +383,52 @@ __device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const D
     float2 hY = fma2(bc2(-P.Liso), lapY, make_float2(h[3], h[4]));
     float hzz = fmaf(P.Liso, lapX.x + lapX.y, h[2]);  // - Liso lap_zz, lap_zz = -(lap_xx + lap_yy)
     float hyz = fmaf(-P.Liso, lapZ, h[5]);
+    // undivided mixed second differences (four corners) of every component: (xx, yy), (xy, xz), yz
+    float2 mxyX{}, mxzX{}, myzX{}, mxyY{}, mxzY{}, myzY{};
+    float mxyZ = 0.0f, mxzZ = 0.0f, myzZ = 0.0f;
+    if (kMixed) {
+        mxyX = sub2(sub2(X(1, 1, 0), X(1, -1, 0)), sub2(X(-1, 1, 0), X(-1, -1, 0)));
+        mxzX = sub2(sub2(X(1, 0, 1), X(1, 0, -1)), sub2(X(-1, 0, 1), X(-1, 0, -1)));
+        myzX = sub2(sub2(X(0, 1, 1), X(0, 1, -1)), sub2(X(0, -1, 1), X(0, -1, -1)));
+        mxyY = sub2(sub2(Y(1, 1, 0), Y(1, -1, 0)), sub2(Y(-1, 1, 0), Y(-1, -1, 0)));
+        mxzY = sub2(sub2(Y(1, 0, 1), Y(1, 0, -1)), sub2(Y(-1, 0, 1), Y(-1, 0, -1)));
+        myzY = sub2(sub2(Y(0, 1, 1), Y(0, 1, -1)), sub2(Y(0, -1, 1), Y(0, -1, -1)));
+        mxyZ = (Z(1, 1, 0) - Z(1, -1, 0)) - (Z(-1, 1, 0) - Z(-1, -1, 0));
+        mxzZ = (Z(1, 0, 1) - Z(1, 0, -1)) - (Z(-1, 0, 1) - Z(-1, 0, -1));
+        myzZ = (Z(0, 1, 1) - Z(0, 1, -1)) - (Z(0, -1, 1) - Z(0, -1, -1));
+    }
     if (kL2) {
-        // h -= L2 d_a D_b (central differences of the staged column divergence, QSR.cu:436-460)
-        hX = fma2(make_float2(-P.L2i2x, -P.L2i2y),
-                  sub2(make_float2(DA(0, 1, 0, 0), DA(1, 0, 1, 0)), make_float2(DA(0, -1, 0, 0), DA(1, 0, -1, 0))), hX);
-        hY = fma2(bc2(-P.L2i2x),
-                  sub2(make_float2(DA(1, 1, 0, 0), DA(2, 1, 0, 0)), make_float2(DA(1, -1, 0, 0), DA(2, -1, 0, 0))), hY);
-        hY = fma2(make_float2(-P.L2i2y, -P.L2i2z),
-                  sub2(make_float2(DA(0, 0, 1, 0), DA(0, 0, 0, 1)), make_float2(DA(0, 0, -1, 0), DA(0, 0, 0, -1))), hY);
-        hzz = fmaf(-P.L2i2z, DA(2, 0, 0, 1) - DA(2, 0, 0, -1), hzz);
-        hyz = fmaf(-P.L2i2y, DA(2, 0, 1, 0) - DA(2, 0, -1, 0), hyz);
-        hyz = fmaf(-P.L2i2z, DA(1, 0, 0, 1) - DA(1, 0, 0, -1), hyz);
+        // wide second differences Q(+2a) - 2 Q + Q(-2a) of the components d_a D_b needs
+        const float q2xx = 2.0f * q[0], q2xy = 2.0f * q[1], q2xz = 2.0f * q[2], q2yy = 2.0f * q[3],
+                    q2yz = 2.0f * q[4];
+        const float wx_xx = (A(0, 2, 0, 0) + A(0, -2, 0, 0)) - q2xx;
+        const float wx_xy = (A(1, 2, 0, 0) + A(1, -2, 0, 0)) - q2xy;
+        const float wx_xz = (A(2, 2, 0, 0) + A(2, -2, 0, 0)) - q2xz;
+        const float wy_yy = (A(3, 0, 2, 0) + A(3, 0, -2, 0)) - q2yy;
+        const float wy_xy = (A(1, 0, 2, 0) + A(1, 0, -2, 0)) - q2xy;
+        const float wy_yz = (A(4, 0, 2, 0) + A(4, 0, -2, 0)) - q2yz;
+        const float wz_xx = (A(0, 0, 0, 2) + A(0, 0, 0, -2)) - q2xx;
+        const float wz_yy = (A(3, 0, 0, 2) + A(3, 0, 0, -2)) - q2yy;
+        const float wz_xz = (A(2, 0, 0, 2) + A(2, 0, 0, -2)) - q2xz;
+        const float wz_yz = (A(4, 0, 0, 2) + A(4, 0, 0, -2)) - q2yz;
+        const float wz_zz = -(wz_xx + wz_yy);
+        const float mxz_zz = -(mxzX.x + mxzX.y), myz_zz = -(myzX.x + myzX.y);
+        const float cxx = P.l2w[0], cyy = P.l2w[1], czz = P.l2w[2], cxy = P.l2w[3], cxz = P.l2w[4], cyz = P.l2w[5];
+        // d_x D_x, d_y D_y, d_z D_z
+        const float dxDx = fmaf(cxx, wx_xx, fmaf(cxy, mxyY.x, cxz * mxzY.y));
+        const float dyDy = fmaf(cxy, mxyY.x, fmaf(cyy, wy_yy, cyz * myzZ));
+        const float dzDz = fmaf(cxz, mxzY.y, fmaf(cyz, myzZ, czz * wz_zz));
+        // mixed: d_x D_y + d_y D_x, d_x D_z + d_z D_x, d_y D_z + d_z D_y
+        const float sxy = fmaf(cxx, wx_xy, fmaf(cxy, mxyX.y, fmaf(cxz, mxzZ,
+                          fmaf(cxy, mxyX.x, fmaf(cyy, wy_xy, cyz * myzY.y)))));
+        const float sxz = fmaf(cxx, wx_xz, fmaf(cxy, mxyZ, fmaf(cxz, mxz_zz,
+                          fmaf(cxz, mxzX.x, fmaf(cyz, myzY.x, czz * wz_xz)))));
+        const float syz = fmaf(cxy, mxyY.y, fmaf(cyy, wy_yz, fmaf(cyz, myz_zz,
+                          fmaf(cxz, mxzY.x, fmaf(cyz, myzX.y, czz * wz_yz)))));
+        hX = fma2(bc2(-1.0f), make_float2(dxDx, dyDy), hX);
+        hY = fma2(bc2(-1.0f), make_float2(sxy, sxz), hY);
+        hzz -= dzDz;
+        hyz -= syz;
     }
     float corr = (hX.x + hX.y + hzz) * (1.0f / 3.0f);
     float2 muX = add2(hX, bc2(-corr));  // (mu_xx, mu_yy)
@@ -408,41 +452,24 @@ __device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const D
         float hxy = fmaf(P.l3m[3], M(dXx, dXy, dYx, dYy2, dZx, dZy, d5x, d5y), muY.x);
         float hxz = fmaf(P.l3m[4], M(dXx, dXz, dYx, dYz2, dZx, dZz, d5x, d5z), muY.y);
         float hyz3 = fmaf(P.l3m[5], M(dXy, dXz, dYy, dYz2, dZy, dZz, d5y, d5z), muZ);
+        // column divergence at the centre: D_x = d_x Q_xx + d_y Q_xy + d_z Q_xz, ... (QSR.cu:325-371)
+        const float Dx = fmaf(P.i2x, dXx.x, fmaf(P.i2y, dYy.x, P.i2z * dYz.y));
+        const float Dy = fmaf(P.i2x, dYx.x, fmaf(P.i2y, dXy.y, P.i2z * dZz));
+        const float Dz = fmaf(P.i2x, dYx.y, fmaf(P.i2y, dZy, P.i2z * d5z));
         // B(Q_c) = D . grad Q_c + Q_ab d_a d_b Q_c (QSR.cu:580-603) on all components at once:
         // weights of the six second derivatives, shared by every component
         const float Qzz = -q[0] - q[3];
         const float2 wxx = bc2(q[0] * P.ix2), wyy = bc2(q[3] * P.iy2), wzz = bc2(Qzz * P.iz2);
         const float2 wxy = bc2(2.0f * q[1] * P.i4xy), wxz = bc2(2.0f * q[2] * P.i4xz), wyz = bc2(2.0f * q[4] * P.i4yz);
-        const float2 Dc0 = bc2(DA(0, 0, 0, 0) * P.i2x), Dc1 = bc2(DA(1, 0, 0, 0) * P.i2y),
-                     Dc2 = bc2(DA(2, 0, 0, 0) * P.i2z);
-        auto mixedX = [&](int a, int b) {
-            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
-            pa[a] = 1; pb[b] = 1;
-            return sub2(sub2(X(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]), X(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])),
-                        sub2(X(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]),
-                             X(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2])));
-        };
-        auto mixedY = [&](int a, int b) {
-            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
-            pa[a] = 1; pb[b] = 1;
-            return sub2(sub2(Y(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]), Y(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])),
-                        sub2(Y(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]),
-                             Y(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2])));
-        };
-        auto mixedZ = [&](int a, int b) {
-            int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
-            pa[a] = 1; pb[b] = 1;
-            return (Z(pa[0] + pb[0], pa[1] + pb[1], pa[2] + pb[2]) - Z(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2])) -
-                   (Z(-pa[0] + pb[0], -pa[1] + pb[1], -pa[2] + pb[2]) - Z(-pa[0] - pb[0], -pa[1] - pb[1], -pa[2] - pb[2]));
-        };
+        const float2 Dc0 = bc2(Dx * P.i2x), Dc1 = bc2(Dy * P.i2y), Dc2 = bc2(Dz * P.i2z);
         const float2 q2X = add2(qX, qX), q2Y = add2(qY, qY);
         const float2 cX = fma2(wxx, sub2(sxX, q2X), fma2(wyy, sub2(syX, q2X), fma2(wzz, sub2(szX, q2X),
-                          fma2(wxy, mixedX(0, 1), fma2(wxz, mixedX(0, 2), mul2(wyz, mixedX(1, 2)))))));
+                          fma2(wxy, mxyX, fma2(wxz, mxzX, mul2(wyz, myzX))))));
         const float2 cY = fma2(wxx, sub2(sxY, q2Y), fma2(wyy, sub2(syY, q2Y), fma2(wzz, sub2(szY, q2Y),
-                          fma2(wxy, mixedY(0, 1), fma2(wxz, mixedY(0, 2), mul2(wyz, mixedY(1, 2)))))));
+                          fma2(wxy, mxyY, fma2(wxz, mxzY, mul2(wyz, myzY))))));
         const float q2Z = 2.0f * qZ;
         const float cZ = fmaf(wxx.x, sxZ - q2Z, fmaf(wyy.x, syZ - q2Z, fmaf(wzz.x, szZ - q2Z,
-                         fmaf(wxy.x, mixedZ(0, 1), fmaf(wxz.x, mixedZ(0, 2), wyz.x * mixedZ(1, 2))))));
+                         fmaf(wxy.x, mxyZ, fmaf(wxz.x, mxzZ, wyz.x * myzZ)))));
         const float2 BX = fma2(Dc0, dXx, fma2(Dc1, dXy, fma2(Dc2, dXz, cX)));  // (B_xx, B_yy)
         const float2 BY = fma2(Dc0, dYx, fma2(Dc1, dYy, fma2(Dc2, dYz, cY)));  // (B_xy, B_xz)
         const float BZ = fmaf(Dc0.x, dZx, fmaf(Dc1.x, dZy, fmaf(Dc2.x, dZz, cZ)));  // B_yz

@@ -654,6 +654,7 @@ QsrConst make_const(const qsr_handle* h, double T, double S_shell, double dt) {
     const double i2[3] = {1.0 / (2.0 * p.dx), 1.0 / (2.0 * p.dy), 1.0 / (2.0 * p.dz)};
     const int ab[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
     for (int m = 0; m < 6; ++m) P.l3m[m] = (float)(0.5 * p.L3 * i2[ab[m][0]] * i2[ab[m][1]]);
+    for (int m = 0; m < 6; ++m) P.l2w[m] = (float)(p.L2 * i2[ab[m][0]] * i2[ab[m][1]]);
     return P;
 }
 

@@ -4,13 +4,20 @@
 // of planes. Each plane of the input field arrives in shared memory through one TMA load
 // of a 4-D box (k, j, i, component) covering the tile plus a halo of 2 rows and 4 columns
 // (the k start stays on a 16-byte boundary), so every Q value is read from HBM about once.
-// The ring holds the planes i-2 .. i+3 plus the planes in flight. The column divergence D
-// (needed by the L2 and L3 terms) is computed once per plane, one plane ahead, on the tile
-// plus a 1-cell halo into a 4-plane shared ring, so each plane costs one CTA barrier. Per cell the kernel then evaluates the chemical potential and
-// the update from shared memory and writes only the cells that change (moving and strongly
-// anchored cells): frozen exterior cells hold identical values in both ping-pong buffers.
-// Tiles that contain no changing cell are never visited (host-built work list). The same
-// per-tile routine drives a persistent, work-stealing ensemble kernel over many droplets.
+// The ring holds the planes i-2 .. i+2 that the cells of plane i read, plus planes in flight.
+// Interior cells read only Q: the L2 term's derivatives of the column divergence are
+// evaluated from Q directly (wide and four-corner second differences, which for an interior
+// cell equal the reference's central differences of its central divergence), so no divergence
+// field is staged and the warps share nothing but the plane ring. Each warp (one tile row)
+// therefore marches on its own: it waits only for the TMA of the planes it reads, and when it
+// is done with a plane it arrives on that slot's counter; the warp whose arrival completes the
+// count issues the load of the plane that reuses the slot. There is no CTA barrier per plane.
+// Cells next to a grid face take the reference's face stencils with the divergence evaluated on
+// the fly. Per cell the kernel evaluates the chemical potential and the update from shared memory
+// and writes only the cells that change (moving and strongly anchored cells): frozen exterior
+// cells hold identical values in both ping-pong buffers. Tiles that contain no changing cell are
+// never visited (host-built work list). The same per-tile routine drives a persistent,
+// work-stealing ensemble kernel over many droplets.
 //
 // mbarrier waits are bounded: on timeout the kernel records LDG_ERR_TIMEOUT in a device
 // word, waits (bounded) for its own TMA loads and returns.
@@ -35,21 +42,23 @@ namespace tiled {
 constexpr int TK = 32;               // tile width along k (one warp per row)
 constexpr int TJ = 8;                // tile rows along j (one warp each)
 constexpr int THREADS = TK * TJ;
+constexpr int NWARP = THREADS / 32;
 constexpr int HJ = 2, HK = 4;        // halo rows / columns loaded with each plane
 constexpr int RW = TK + 2 * HK;      // 40 floats per smem row
 constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
 constexpr int CSTR = RW * ROWS;      // floats per component plane
 constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
-// Q ring slots: planes i-2 .. i+3 in use at plane i, plane i+4 in flight (issued at the end of
-// plane i). Six slots keep a CTA at ~74 KB of shared memory with the divergence ring, so three
-// CTAs (24 warps) fit on an SM, with the registers capped by the launch bounds below.
-constexpr int NQ = 6;
-constexpr int DRW = TK + 2, DROWS = TJ + 2;
-constexpr int DCSTR = DRW * DROWS;
-constexpr int DPLANE = 3 * DCSTR;
-constexpr int NDS = 4;               // D ring slots: D(i-1) .. D(i+2)
+constexpr int LOOK = 2;              // the cells of plane i read planes i-2 .. i+2
+// Q ring slots: planes i-2 .. i+2 read at plane i, planes i+3 and i+4 in flight. ~67 KB of
+// shared memory per CTA, so three CTAs (24 warps) fit on an SM, with the registers capped by the
+// launch bounds below.
+constexpr int NQ = 7;
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
 constexpr int CHUNK = 16;            // planes per work item (default; tunable)
+// CTAs per SM the step kernels are compiled for (caps registers at 65536 / (256 x this)).
+#ifndef LDG_TILED_CTAS_PER_SM
+#define LDG_TILED_CTAS_PER_SM 3
+#endif
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -108,39 +117,53 @@ struct SmemQ {
     }
 };
 
-// Shared-memory D accessor centred on local cell (jl, kl) of plane i; planes i-1..i+1.
-struct SmemD {
-    const float* pl[3];
-    int off;
+// Column divergence D_comp at offset (di, dj, dk) of cell (i, j, k), evaluated on the fly from a
+// Q accessor with the reference's face stencils (QSR.cu:325-371): the face path of the tiled kernel.
+template <class Acc>
+struct FlyD {
+    const Acc* A;
+    const QsrConst* P;
+    int i, j, k;
     __device__ __forceinline__ float operator()(int comp, int di, int dj, int dk) const {
-        return pl[di + 1][off + comp * DCSTR + dj * DRW + dk];
+        float D[3];
+        dcol_at(*A, *P, i, j, k, di, dj, dk, D);
+        return D[comp];
     }
 };
 
 // Shared-memory layout of one CTA of the tiled kernels.
 struct TileSmem {
-    float* sq;       // NQ planes of Q (tile + halo, 5 components)
-    float* sd;       // NDS planes of the column divergence
-    uint64_t* bar;   // NQ mbarriers, one per Q slot
-    int* s_abort;    // set when a bounded wait gave up
-    int* s_item;     // work item broadcast (persistent kernel)
+    float* sq;          // NQ planes of Q (tile + halo, 5 components)
+    uint64_t* bar;      // NQ mbarriers, one per Q slot (TMA completion)
+    unsigned* freed;    // NQ counters of warps done with the slot's plane
+    int* s_abort;       // set when a bounded wait gave up
+    int* s_item;        // work item broadcast (persistent kernel)
 };
 
-template <bool kD>
 __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
     TileSmem S;
     S.sq = reinterpret_cast<float*>(raw);
-    S.sd = S.sq + NQ * PLANE;
-    S.bar = reinterpret_cast<uint64_t*>(S.sd + (kD ? NDS * DPLANE : 0));
-    S.s_abort = reinterpret_cast<int*>(S.bar + NQ);
+    S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * PLANE);
+    S.freed = reinterpret_cast<unsigned*>(S.bar + NQ);
+    S.s_abort = reinterpret_cast<int*>(S.freed + NQ);
     S.s_item = S.s_abort + 1;
     return S;
+}
+constexpr size_t TILE_SMEM_BYTES = (size_t)NQ * PLANE * 4 + NQ * 8 + NQ * 4 + 16;
+
+// A warp's arrival on a slot counter: returns the count before it (acquire-release at CTA
+// scope, so the warp's reads of the plane happen before the slot is refilled).
+__device__ __forceinline__ unsigned arrive_freed(unsigned* ctr) {
+    unsigned old;
+    asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], 1;" : "=r"(old) : "r"(su32(ctr)) : "memory");
+    return old;
 }
 
 // One work item: the (TJ x TK) column tile at (j0, k0) over planes [ib, ie). `phase` holds the
 // parity of the next phase of every slot barrier (bit s for slot s), so a CTA can run many
-// items in a row; every load the item issues is waited for before it returns. Returns false
-// when a bounded wait gave up (the CTA must stop).
+// items in a row; every load the item issues is waited for by every warp before it returns.
+// Returns false when a bounded wait gave up (the CTA must stop). The caller synchronises the CTA
+// before and after an item.
 // kComp: compensated storage (explicit steps only): the low words of the input cells are read
 // from lo_in and the new low words written to lo_out.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
@@ -149,20 +172,14 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                                              const QsrConst& P, const TileSmem& S, uint32_t& phase,
                                              int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
                                              float* __restrict__ lo_out = nullptr) {
-    constexpr bool kD = kL2 || kL3;
-    // Plane lookahead: with the divergence, step i computes D(i+2), which reads Q(i+3).
-    constexpr int LOOK = kD ? 3 : 2;
     float* sq = S.sq;
-    float* sd = S.sd;
     uint64_t* bar = S.bar;
     const int base = ib - 2;  // first plane this item loads; slots and phases count from it
     const int tid = threadIdx.x;
-    const int kl = tid & (TK - 1), jl = tid / TK;
+    const int kl = tid & 31, jl = tid >> 5;
 
     // Plane p (p >= base) lives in slot (p - base) % NQ and completes that slot's barrier phase
-    // number (p - base) / NQ of this item.
-    // (every caller has p >= base, so the ring arithmetic is unsigned; a few times per plane)
-    static_assert(NQ >= 6, "planes i-2 .. i+3 are read at plane i");
+    // number (p - base) / NQ of this item (every caller has p >= base: unsigned arithmetic).
     auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
     auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
 
@@ -171,178 +188,120 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     auto issue = [&](int p) {
         uint64_t* b = &bar[slot(p)];
         if (p >= 0 && p < P.Nx && p < ie + LOOK) {
+            fence_proxy_async();
             mbar_expect_tx(b, PLANE_BYTES);
             tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
             mbar_arrive(b);
         }
     };
-    int issued_end = base + NQ;  // planes [base, issued_end) issued (same value in every thread)
-    if (tid == 0) {
-        fence_proxy_async();
+    if (tid == 0)
         for (int p = base; p < base + NQ; ++p) issue(p);
-    }
-    int waited_end = base;  // planes [base, waited_end) waited for
     bool ok = true;
     auto wait_plane = [&](int p) {
         if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
             atomicExch(err, LDG_ERR_TIMEOUT);
-            *S.s_abort = 1;
+            *(volatile int*)S.s_abort = 1;
             ok = false;
         }
-        waited_end = p + 1;
     };
-
-    // The tile plus its 2-cell halo lies strictly inside the grid in j and k: planes with
-    // 2 <= i <= Nx-3 then need no face stencils anywhere (cells, divergence halo, L3).
-    const bool tile_interior = (j0 >= 2) && (j0 + TJ + 2 <= P.Ny) && (k0 >= 2) && (k0 + TK + 2 <= P.Nz);
-    // Column divergence of plane p on the tile plus a 1-cell halo into D slot p % NDS.
-    // Reads Q planes p-1 .. p+1 (all waited for by the caller).
-    // Work split: warp w computes columns 0..31 of D rows w, w + 8, ... (a warp never spans two
-    // rows, so its shared-memory accesses are bank-conflict free); the two remaining columns of
-    // every row (2 x DROWS cells) go to the warp that has one row fewer, DROWS % 8.
-    static_assert(DRW == 32 + 2 && 2 * DROWS <= 32, "D tile = 32 + 2 columns, one spare warp");
-    constexpr int NWARP = THREADS / 32, SPARE = DROWS % NWARP;
-    // pm, pc, pp: the shared-memory Q planes p-1, p, p+1 (the first derivatives reach no
-    // further); dst: the D slot of plane p.
-    auto compute_D = [&](int p, const float* pm, const float* pc, const float* pp, float* dst) {
-        if (p < 0 || p >= P.Nx) return;
-        SmemQ A;
-        A.pl[0] = pm; A.pl[1] = pm; A.pl[2] = pc; A.pl[3] = pp; A.pl[4] = pp;
-        const int lane = tid & 31, warp = tid >> 5;
-        const bool face_free = tile_interior && p >= 1 && p <= P.Nx - 2;
-        auto one = [&](int r, int cidx) {
-            const int t = r * DRW + cidx;
-            const int j = j0 + r - 1, k = k0 + cidx - 1;
-            float D[3] = {0.0f, 0.0f, 0.0f};
-            A.off = (r - 1 + HJ) * RW + (cidx - 1 + HK);
-            if (face_free)
-                dcol_at<false>(A, P, p, j, k, 0, 0, 0, D);
-            else if (j >= 0 && j < P.Ny && k >= 0 && k < P.Nz)
-                dcol_at(A, P, p, j, k, 0, 0, 0, D);
-            dst[t] = D[0];
-            dst[DCSTR + t] = D[1];
-            dst[2 * DCSTR + t] = D[2];
-        };
-        for (int r = warp; r < DROWS; r += NWARP) one(r, lane);
-        if (warp == SPARE && lane < 2 * DROWS) one(lane >> 1, 32 + (lane & 1));
-    };
-
-    // Prologue: planes ib-2 .. ib+LOOK-1, then D(ib-1) .. D(ib+1) (visible after the barrier).
-    for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
-    __syncthreads();
-    auto qplane = [&](int p) { return sq + slot(p) * PLANE; };
-    auto dslot = [&](int p) { return sd + ((uint32_t)(p + NDS) % (uint32_t)NDS) * DPLANE; };
-    if (kD && !*S.s_abort) {
-        for (int p = ib - 1; p <= ib + 1; ++p) compute_D(p, qplane(p - 1), qplane(p), qplane(p + 1), dslot(p));
-    }
-    __syncthreads();
+    // Planes [base, ie + NQ - 2) are issued: the first NQ here, then plane p + NQ when the last
+    // warp is done with plane p (after its plane p + 2), for every p <= ie - 3.
+    const int issued_end = ie + NQ - 2;
 
     const int j = j0 + jl, k = k0 + kl;
     const bool in_grid = (j < P.Ny) && (k < P.Nz);
-    // Cells with 1 <= j <= Ny-2 and 1 <= k <= Nz-2 (and 1 <= i <= Nx-2) need no face stencil.
-    const bool jk_interior = j >= 1 && j <= P.Ny - 2 && k >= 1 && k <= P.Nz - 2;
-    // The classification of plane i+1 is fetched while plane i is computed (its global-load
-    // latency is then off the critical path).
+    // Interior cells take the Q-only path: every stencil position within the grid away from the
+    // faces (the L2 term reaches two cells out: 2 <= pos <= N - 3; otherwise 1 <= pos <= N - 2).
+    constexpr int kLo = kL2 ? 2 : 1;
+    const bool jk_interior = j >= kLo && j <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
     const long long cell0 = (long long)j * P.sj + k;
     uint8_t f_next = in_grid ? __ldg(flags + (long long)ib * P.si + cell0) : 0;
-    // Shared-memory planes of the current step, rolled forward by one plane per step:
-    // Q planes i-2 .. i+3 (the cells read i-2 .. i+2, D(i+2) reads i+1 .. i+3) and divergence
-    // slots i-1 .. i+2 (the cells read i-1 .. i+1, D(i+2) is written; the four slots rotate).
-    const float* qpl[6];
-    float* dpl[NDS];
-    static_assert(NDS == 4, "divergence slots i-1 .. i+2");
+    // Shared-memory planes i-2 .. i+2 of the current step, rolled forward by one plane per step.
+    const float* qpl[5];
 #pragma unroll
-    for (int d = 0; d < 6; ++d) qpl[d] = qplane(ib + d - 2);
-#pragma unroll
-    for (int d = 0; d < NDS; ++d) dpl[d] = dslot(ib + d - 1);
-    // One barrier per plane: D(i+2) is written into the slot of D(i-2) (last read in step i-1)
-    // while the cells of plane i read D(i-1) .. D(i+1), all written before the last barrier.
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+    int waited_end = base;
+    for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
+    waited_end = ib + LOOK;
     for (int i = ib; i < ie; ++i) {
-        if (*S.s_abort) break;  // uniform: read after a barrier
+        if (*(volatile int*)S.s_abort) { ok = false; break; }  // another warp gave up
         const uint8_t f = f_next;
         if (in_grid && i + 1 < ie) f_next = __ldg(flags + (long long)(i + 1) * P.si + cell0);
         wait_plane(i + LOOK);
-        if (kD) compute_D(i + 2, qpl[3], qpl[4], qpl[5], dpl[3]);
+        waited_end = i + LOOK + 1;
+        if (!ok) break;
         const bool fixed = in_grid && !kRHS && (f & kFixed);
         const bool move = in_grid && (f & kMove) != 0;
-        // The face-free form is taken by a whole warp when none of its computing cells touches a
-        // face (exterior cells of a droplet compute nothing, so small droplets use it too).
+        // The Q-only interior form is taken by a whole warp when none of its computing cells is
+        // near a face (exterior cells of a droplet compute nothing, so small droplets use it too).
         const bool warp_interior =
-            __all_sync(0xffffffffu, !move || (jk_interior && i >= 1 && i <= P.Nx - 2)) != 0;
-        if (in_grid) {
+            __all_sync(0xffffffffu, !move || (jk_interior && i >= kLo && i <= P.Nx - 1 - kLo)) != 0;
+        if (fixed || move) {
             const long long id = (long long)i * P.si + cell0;
-            if (fixed || move) {
-                SmemQ A;
+            SmemQ A;
 #pragma unroll
-                for (int d = 0; d < 5; ++d) A.pl[d] = qpl[d];
-                A.off = (jl + HJ) * RW + (kl + HK);
-                float c[5], o[5];
+            for (int d = 0; d < 5; ++d) A.pl[d] = qpl[d];
+            A.off = (jl + HJ) * RW + (kl + HK);
+            float c[5], o[5];
 #pragma unroll
-                for (int m = 0; m < 5; ++m) c[m] = A(m, 0, 0, 0);
-                if (fixed) {
-                    surface_q0(P, i, j, k, o);
-                    if (kComp) {
+            for (int m = 0; m < 5; ++m) c[m] = A(m, 0, 0, 0);
+            if (fixed) {
+                surface_q0(P, i, j, k, o);
+                if (kComp) {
 #pragma unroll
-                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
-                    }
-                } else {
-                    SmemD DA;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) DA.pl[d] = dpl[d];
-                    DA.off = (jl + 1) * DRW + (kl + 1);
-                    float mu[5], lap[5];
-                    if (warp_interior)
-                        chem_potential_interior_x2<kL2, kL3>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
-                    else
-                        chem_potential<kL2, kL3, true>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
-                    const uint32_t cell = (uint32_t)(k + P.Nz * (j + P.Ny * i));
-                    if (kRHS) {
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) o[m] = c[m] - P.mob_dt * mu[m] - P.alpha * lap[m];
-                        if (kNoise) {
-                            float g[5];
-                            normals5(cell, P.instance, P.step, P.key0, P.key1, g);
-#pragma unroll
-                            for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
-                        }
-                    } else if (kComp) {
-                        float lo[5];
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
-                        euler_update_comp(P, c, lo, mu, cell, kNoise, o);
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
-                    } else {
-                        euler_update(P, c, mu, cell, kNoise, o);
-                    }
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
                 }
+            } else {
+                float mu[5], lap[5];
+                if (warp_interior) {
+                    chem_potential_interior_x2<kL2, kL3>(A, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                } else {
+                    const FlyD<SmemQ> DA{&A, &P, i, j, k};
+                    chem_potential<kL2, kL3, true>(A, DA, P, i, j, k, c, (f & kAnchor) != 0, mu, lap);
+                }
+                const uint32_t cell = (uint32_t)(k + P.Nz * (j + P.Ny * i));
+                if (kRHS) {
 #pragma unroll
-                for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
+                    for (int m = 0; m < 5; ++m) o[m] = c[m] - P.mob_dt * mu[m] - P.alpha * lap[m];
+                    if (kNoise) {
+                        float g[5];
+                        normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
+                    }
+                } else if (kComp) {
+                    float lo[5];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
+                    euler_update_comp(P, c, lo, mu, cell, kNoise, o);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
+                } else {
+                    euler_update(P, c, mu, cell, kNoise, o);
+                }
             }
-        }
-        __syncthreads();
-        // Plane i-2 is dead: its slot takes plane i-2+NQ.
-        if (tid == 0) {
-            fence_proxy_async();
-            issue(issued_end);
-        }
-        ++issued_end;
 #pragma unroll
-        for (int d = 0; d < 5; ++d) qpl[d] = qpl[d + 1];
-        qpl[5] = qplane(i + 4);
-        float* const d0 = dpl[0];  // slot of D(i-1) takes D(i+3)
+            for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
+        }
+        // This warp is done with plane i-2: arrive on its slot; the last warp refills the slot with
+        // plane i-2+NQ.
+        __syncwarp();
+        if (kl == 0) {
+            const uint32_t s = slot(i - 2);
+            if (arrive_freed(&S.freed[s]) % (unsigned)NWARP == (unsigned)NWARP - 1u) issue(i - 2 + NQ);
+        }
 #pragma unroll
-        for (int d = 0; d < NDS - 1; ++d) dpl[d] = dpl[d + 1];
-        dpl[NDS - 1] = d0;
+        for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
+        qpl[4] = sq + slot(i + 3) * PLANE;
     }
-    // Drain: every load this item issued lands before the slots are reused or released.
-    for (int p = waited_end; p < issued_end; ++p) {
-        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
-            atomicExch(err, LDG_ERR_TIMEOUT);
-            *S.s_abort = 1;
-            ok = false;
-        }
+    // Drain: every load this item issues lands before the slots are reused or released. After
+    // an abort some refills are never issued; those waits give up after their bound.
+    if (ok) {
+        for (int p = waited_end; p < issued_end; ++p) wait_plane(p);
+    } else {
+        for (int p = waited_end; p < issued_end; ++p)
+            if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) break;
     }
     // Advance the per-slot phase parities by the number of loads each slot received.
     const int n_issued = issued_end - base;
@@ -354,26 +313,27 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     return ok;
 }
 
-template <bool kD>
 __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NQ; ++s) mbar_init(&S.bar[s], 1);
+        for (int s = 0; s < NQ; ++s) {
+            mbar_init(&S.bar[s], 1);
+            S.freed[s] = 0;
+        }
         mbar_fence_init();
         *S.s_abort = 0;
     }
     __syncthreads();
 }
 
-// Single grid: one work item per CTA; three CTAs per SM (the bounds cap registers at 80).
+// Single grid: one work item per CTA.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
-__global__ void __launch_bounds__(THREADS, 3)
+__global__ void __launch_bounds__(THREADS, LDG_TILED_CTAS_PER_SM)
     k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
                  const int4* __restrict__ items, QsrConst P, int* __restrict__ err, const float* __restrict__ lo_in,
                  float* __restrict__ lo_out) {
-    constexpr bool kD = kL2 || kL3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const TileSmem S = tile_smem<kD>(smem_raw);
-    tile_smem_init<kD>(S);
+    const TileSmem S = tile_smem(smem_raw);
+    tile_smem_init(S);
     const int4 item = items[blockIdx.x];
     uint32_t phase = 0;
     process_tile<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase, err,
@@ -437,13 +397,12 @@ __host__ __device__ __forceinline__ double ens_S_eq(double A, double B, double C
 }
 
 template <bool kL2, bool kL3, bool kNoise>
-__global__ void __launch_bounds__(THREADS, 3)
+__global__ void __launch_bounds__(THREADS, LDG_TILED_CTAS_PER_SM)
     k_step_ensemble(const CUtensorMap* __restrict__ tms, const EnsInstDev* __restrict__ inst,
                     const EnsItem* __restrict__ items, int n_items, EnsCtl* __restrict__ ctl, int* __restrict__ err) {
-    constexpr bool kD = kL2 || kL3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const TileSmem S = tile_smem<kD>(smem_raw);
-    tile_smem_init<kD>(S);
+    const TileSmem S = tile_smem(smem_raw);
+    tile_smem_init(S);
     // Every CTA reads the step index before any CTA of this launch finishes (the last CTA to
     // finish advances it).
     const long long step = *((volatile long long*)&ctl->step);
@@ -600,8 +559,8 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     if (rc) return rc;
     plan.bufs[0] = buf0;
     plan.bufs[1] = buf1;
-    plan.smem_bytes[0] = (size_t)NQ * PLANE * 4 + NQ * 8 + 16;
-    plan.smem_bytes[1] = (size_t)NQ * PLANE * 4 + (size_t)NDS * DPLANE * 4 + NQ * 8 + 16;
+    plan.smem_bytes[0] = TILE_SMEM_BYTES;
+    plan.smem_bytes[1] = TILE_SMEM_BYTES;
     plan.ok = true;
     return LDG_OK;
 }
@@ -610,8 +569,7 @@ template <bool L2, bool L3, bool N, bool R, bool K>
 inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const uint8_t* flags, const QsrConst& P,
                           cudaStream_t st, const float* lo_in, float* lo_out) {
     using namespace tiled;
-    constexpr bool kD = L2 || L3;
-    const size_t smem = plan.smem_bytes[kD ? 1 : 0];
+    const size_t smem = plan.smem_bytes[(L2 || L3) ? 1 : 0];
     static bool configured = false;
     if (!configured) {
         LDG_CUDA(cudaFuncSetAttribute(k_step_tiled<L2, L3, N, R, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,

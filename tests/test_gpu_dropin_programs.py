@@ -214,7 +214,7 @@ def test_guards_exit_like_reference(tmp_path):
     o = run_both("qsr", "sim_mode = 1\nNx = 16\nNy = 16\nNz = 16\nT = 300\nT_star = 307\nL1 = 6e-12\n", tmp_path)
     assert o["ref"][0].returncode == 1 and o["ours"][0].returncode == 1
     # instability abort of the quench loop (S_abort)
-    cfg = QSR_QUENCH.format(imex="n").replace("total_iters = 200", "total_iters = 100") + "S_abort = 0.01\n"
+    cfg = QSR_QUENCH.format(imex="n").replace("total_iters = 200", "total_iters = 100") + "S_abort = 0.001\n"
     o = run_both("qsr", cfg, tmp_path / "abort")
     logs = {w: ((o[w][1] / "q" / "quench_log.dat").read_text() if (o[w][1] / "q" / "quench_log.dat").exists()
                 else "") + o[w][0].stderr[-600:] for w in ("ref", "ours")}
