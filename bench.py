@@ -532,6 +532,7 @@ def main():
     chunk = solver.autotune(T, S_shell, dt, trial_steps=10,
                             **({"semi_implicit": True, "L_stab": imex["L_stab"], "jacobi_iters": imex["jacobi"]}
                                if imex else {}))
+    geo = solver.geometry()  # visited cells of the work list at the chosen item length
     for s in range(args.warmup):
         args_step.step_index = s
         solver.step_raw(1, args_step)

@@ -914,7 +914,7 @@ int qsr_geometry(const qsr_handle* h, qsr_geometry_info* o) {
     o->delta_eff = h->delta_eff;
     o->shell_cells = h->shell_cells;
     o->evolving_cells = h->evolving_cells;
-    o->active_cells = h->active_cells;
+    o->active_cells = h->tiled.ok ? h->tiled.active_cells : h->active_cells;
     o->written_cells = h->written_cells;
     o->box_cells = h->ncells;
     return LDG_OK;
@@ -1289,9 +1289,14 @@ void ens_drop_graph(ens_handle* h) {
 // run together share halo planes of one droplet in L2), and the persistent grid size.
 int ens_rechunk(ens_handle* h, int chunk) {
     std::vector<tiled::EnsItem> items;
-    for (size_t n = 0; n < h->inst.size(); ++n)
-        for (const int4& t : tiled_items(h->inst[n]->tiled.cols, chunk))
+    long long active = 0;
+    for (size_t n = 0; n < h->inst.size(); ++n) {
+        long long a = 0;
+        for (const int4& t : tiled_items(h->inst[n]->tiled, chunk, &a))
             items.push_back(tiled::EnsItem{t.x, t.y, t.z, t.w, (int)n, 0, 0, 0});
+        active += a;
+    }
+    h->active = active;
     if (h->d_items) cudaFree(h->d_items);
     h->d_items = nullptr;
     h->n_items = (int)items.size();
