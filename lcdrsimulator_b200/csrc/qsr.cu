@@ -170,18 +170,18 @@ __global__ void __launch_bounds__(256) k_jacobi(const float* __restrict__ rhs, c
 // strongly anchored cells, each over its plane range), writing only moving and strongly anchored
 // cells. Every other cell never changes: it holds the same value in both ping-pong buffers, so
 // the reference's copy of it (QSR.cu:803-810) is already done. Block (32, 8) = one tile row per
-// warp; grid (work items, planes per item): block (x, y) sweeps plane i_begin + y of item x, so
-// every cell is an independent thread as in the full-box sweep.
+// warp; one block per visited tile plane (the work list expanded to single planes), so every
+// cell is an independent thread as in the full-box sweep and no block idles.
 static_assert(tiled::TK == 32 && tiled::TJ == 8, "k_jacobi_tiled maps one (8 x 32) tile onto a 256-thread block");
 template <bool kLast>
 __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ rhs, const float* __restrict__ qo,
                                                       float* __restrict__ qn, const uint8_t* __restrict__ flags,
                                                       const int4* __restrict__ items, QsrConst P) {
     const int4 item = items[blockIdx.x];
-    const int i = item.z + (int)blockIdx.y;
+    const int i = item.z;
     const int k = item.y + (int)(threadIdx.x & 31);
     const int j = item.x + (int)(threadIdx.x >> 5);
-    if (i >= item.w || k >= P.Nz || j >= P.Ny) return;
+    if (k >= P.Nz || j >= P.Ny) return;
     const long long id = (long long)i * P.si + (long long)j * P.sj + k;
     const uint8_t f = __ldg(flags + id);
     if (!(f & (kMove | kFixed))) return;
@@ -1092,14 +1092,14 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             for (int it = 0; it < a->jacobi_iters; ++it) {
                 const bool last = (it == a->jacobi_iters - 1);
                 if (tiled) {
-                    if (h->tiled.n_items > 0) {
-                        const dim3 jg((unsigned)h->tiled.n_items, (unsigned)h->tiled.chunk, 1);
+                    if (h->tiled.n_plane_items > 0) {
+                        const int nb = h->tiled.n_plane_items;
                         if (last)
-                            k_jacobi_tiled<true><<<jg, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                            h->tiled.items, P);
+                            k_jacobi_tiled<true><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                                                                            h->tiled.plane_items, P);
                         else
-                            k_jacobi_tiled<false><<<jg, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                             h->tiled.items, P);
+                            k_jacobi_tiled<false><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                                                                             h->tiled.plane_items, P);
                     }
                 } else if (last) {
                     k_jacobi<true><<<grd, blk, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags, P);

@@ -51,16 +51,14 @@ constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
 constexpr int CSTR = RW * ROWS;      // floats per component plane
 constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
 constexpr int LOOK = 2;              // the cells of plane i read planes i-2 .. i+2
-// Q ring slots: planes i-2 .. i+2 read at plane i, planes i+3 and i+4 in flight. ~67 KB of
-// shared memory per CTA, so three CTAs (24 warps) fit on an SM, with the registers capped by the
-// launch bounds below.
-constexpr int NQ = 7;
+// Q ring slots: planes i-2 .. i+2 are read at plane i, the rest are in flight. The L1-only step
+// runs three CTAs (24 warps) per SM: 7 slots (~67 KB) and at most 80 registers a thread. The
+// L2/L3 steps need more registers (the mixed and wide second differences) and run two CTAs per
+// SM with 9 slots (~86 KB, four planes in flight).
+template <bool kD>
+__host__ __device__ constexpr int nq() { return kD ? 9 : 7; }
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
 constexpr int CHUNK = 16;            // planes per work item (default; tunable)
-// CTAs per SM the step kernels are compiled for (caps registers at 65536 / (256 x this)).
-#ifndef LDG_TILED_CTAS_PER_SM
-#define LDG_TILED_CTAS_PER_SM 3
-#endif
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -75,12 +73,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
 }
+// One bounded try: the thread may sleep in the barrier until the phase completes or the hint
+// (1 ms) runs out, so a waiting warp takes no issue slots from the warps that still compute.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(su32(b)), "r"(parity)
+        : "r"(su32(b)), "r"(parity), "r"(1000000u)
         : "memory");
     return ok != 0;
 }
@@ -135,14 +135,16 @@ struct FlyD {
 
 // Shared-memory layout of one CTA of the tiled kernels.
 struct TileSmem {
-    float* sq;          // NQ planes of Q (tile + halo, 5 components)
-    uint64_t* bar;      // NQ mbarriers, one per Q slot (TMA completion)
-    unsigned* freed;    // NQ counters of warps done with the slot's plane
+    float* sq;          // nq planes of Q (tile + halo, 5 components)
+    uint64_t* bar;      // nq mbarriers, one per Q slot (TMA completion)
+    unsigned* freed;    // nq counters of warps done with the slot's plane
     int* s_abort;       // set when a bounded wait gave up
     int* s_item;        // work item broadcast (persistent kernel)
 };
 
+template <bool kD>
 __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
+    constexpr int NQ = nq<kD>();
     TileSmem S;
     S.sq = reinterpret_cast<float*>(raw);
     S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * PLANE);
@@ -151,7 +153,8 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
     S.s_item = S.s_abort + 1;
     return S;
 }
-constexpr size_t TILE_SMEM_BYTES = (size_t)NQ * PLANE * 4 + NQ * 8 + NQ * 4 + 16;
+template <bool kD>
+__host__ __device__ constexpr size_t tile_smem_bytes() { return (size_t)nq<kD>() * PLANE * 4 + nq<kD>() * 8 + nq<kD>() * 4 + 16; }
 
 // A warp's arrival on a slot counter: returns the count before it (acquire-release at CTA
 // scope, so the warp's reads of the plane happen before the slot is refilled).
@@ -174,6 +177,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
                                              const QsrConst& P, const TileSmem& S, uint32_t& phase,
                                              int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
                                              float* __restrict__ lo_out = nullptr) {
+    constexpr int NQ = nq<kL2 || kL3>();
     float* sq = S.sq;
     uint64_t* bar = S.bar;
     const int base = ib - 2;  // first plane this item loads; slots and phases count from it
@@ -315,9 +319,10 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     return ok;
 }
 
+template <bool kD>
 __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NQ; ++s) {
+        for (int s = 0; s < nq<kD>(); ++s) {
             mbar_init(&S.bar[s], 1);
             S.freed[s] = 0;
         }
@@ -327,15 +332,15 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     __syncthreads();
 }
 
-// Single grid: one work item per CTA.
+// Single grid: one work item per CTA; two CTAs per SM with the L2/L3 terms, three without.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
-__global__ void __launch_bounds__(THREADS, LDG_TILED_CTAS_PER_SM)
+__global__ void __launch_bounds__(THREADS, (kL2 || kL3) ? 2 : 3)
     k_step_tiled(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout, const uint8_t* __restrict__ flags,
                  const int4* __restrict__ items, QsrConst P, int* __restrict__ err, const float* __restrict__ lo_in,
                  float* __restrict__ lo_out) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const TileSmem S = tile_smem(smem_raw);
-    tile_smem_init(S);
+    const TileSmem S = tile_smem<kL2 || kL3>(smem_raw);
+    tile_smem_init<kL2 || kL3>(S);
     const int4 item = items[blockIdx.x];
     uint32_t phase = 0;
     process_tile<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase, err,
@@ -399,12 +404,12 @@ __host__ __device__ __forceinline__ double ens_S_eq(double A, double B, double C
 }
 
 template <bool kL2, bool kL3, bool kNoise>
-__global__ void __launch_bounds__(THREADS, LDG_TILED_CTAS_PER_SM)
+__global__ void __launch_bounds__(THREADS, (kL2 || kL3) ? 2 : 3)
     k_step_ensemble(const CUtensorMap* __restrict__ tms, const EnsInstDev* __restrict__ inst,
                     const EnsItem* __restrict__ items, int n_items, EnsCtl* __restrict__ ctl, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const TileSmem S = tile_smem(smem_raw);
-    tile_smem_init(S);
+    const TileSmem S = tile_smem<kL2 || kL3>(smem_raw);
+    tile_smem_init<kL2 || kL3>(S);
     // Every CTA reads the step index before any CTA of this launch finishes (the last CTA to
     // finish advances it).
     const long long step = *((volatile long long*)&ctl->step);
@@ -462,12 +467,14 @@ struct TiledPlan {
     int n_items = 0;
     int chunk = 0;                // planes per work item (the longest item)
     int4* items = nullptr;        // device work list (j0, k0, i_begin, i_end)
+    int n_plane_items = 0;
+    int4* plane_items = nullptr;  // the same tiles one plane each (j0, k0, i, i + 1): IMEX sweeps
     int Nz = 0;
     std::vector<TiledBand> bands; // host: the changing cells' extent per row band and plane
     int* err = nullptr;           // device error word
     CUtensorMap tmap[2];
     const float* bufs[2] = {nullptr, nullptr};
-    size_t smem_bytes[2] = {0, 0};
+    size_t smem_bytes[2] = {0, 0};  // [L1 only, with L2/L3]
 };
 
 // Work items for chunks of `chunk` planes. In each row band and plane chunk the k tiles start at
@@ -559,6 +566,16 @@ inline int tiled_plan_rechunk(TiledPlan& plan, int chunk) {
         LDG_CUDA(cudaMalloc(&plan.items, items.size() * sizeof(int4)));
         LDG_CUDA(cudaMemcpy(plan.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
     }
+    std::vector<int4> planes;
+    for (const int4& t : items)
+        for (int i = t.z; i < t.w; ++i) planes.push_back(make_int4(t.x, t.y, i, i + 1));
+    if (plan.plane_items) cudaFree(plan.plane_items);
+    plan.plane_items = nullptr;
+    plan.n_plane_items = (int)planes.size();
+    if (plan.n_plane_items > 0) {
+        LDG_CUDA(cudaMalloc(&plan.plane_items, planes.size() * sizeof(int4)));
+        LDG_CUDA(cudaMemcpy(plan.plane_items, planes.data(), planes.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     return LDG_OK;
 }
 
@@ -604,8 +621,8 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     if (rc) return rc;
     plan.bufs[0] = buf0;
     plan.bufs[1] = buf1;
-    plan.smem_bytes[0] = TILE_SMEM_BYTES;
-    plan.smem_bytes[1] = TILE_SMEM_BYTES;
+    plan.smem_bytes[0] = tile_smem_bytes<false>();
+    plan.smem_bytes[1] = tile_smem_bytes<true>();
     plan.ok = true;
     return LDG_OK;
 }
@@ -671,6 +688,7 @@ inline int tiled_check(const TiledPlan& plan, cudaStream_t st) {
 
 inline void tiled_plan_free(TiledPlan& plan) {
     if (plan.items) cudaFree(plan.items);
+    if (plan.plane_items) cudaFree(plan.plane_items);
     cudaFree(plan.err);
     plan = TiledPlan{};
 }
