@@ -492,6 +492,162 @@ __device__ __forceinline__ void chem_potential_interior_x2(const Acc& A, const Q
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Two cells at once: F2 holds one value of two different cells, and every operation on it is
+// one packed instruction (FFMA2 / FADD2 / FMUL2) for both cells. chem_interior_pair is the
+// interior chemical potential of chem_potential_interior_x2 written on F2.
+// ---------------------------------------------------------------------------------------
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 mk2(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2{__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)}; }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 operator*(float s, F2 b) { return F2{__fmul2_rn(make_float2(s, s), b.v)}; }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2{__fmul2_rn(a.v, make_float2(-1.0f, -1.0f))}; }
+__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return F2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ F2 vfma(float a, F2 b, F2 c) { return F2{__ffma2_rn(make_float2(a, a), b.v, c.v)}; }
+
+__device__ __forceinline__ void bulk_field_pair(const F2 q[5], float cQ, float cQ2, float cQ3, F2 h[6]) {
+    const F2 Qxx = q[0], Qxy = q[1], Qxz = q[2], Qyy = q[3], Qyz = q[4];
+    const F2 Qzz = -(Qxx + Qyy);
+    const F2 trQ2 = vfma(Qxx, Qxx, vfma(Qyy, Qyy, Qzz * Qzz)) +
+                    2.0f * vfma(Qxy, Qxy, vfma(Qxz, Qxz, Qyz * Qyz));
+    const F2 q2xx = vfma(Qxx, Qxx, vfma(Qxy, Qxy, Qxz * Qxz));
+    const F2 q2xy = vfma(Qxx, Qxy, vfma(Qxy, Qyy, Qxz * Qyz));
+    const F2 q2xz = vfma(Qxx, Qxz, vfma(Qxy, Qyz, Qxz * Qzz));
+    const F2 q2yy = vfma(Qxy, Qxy, vfma(Qyy, Qyy, Qyz * Qyz));
+    const F2 q2yz = vfma(Qxy, Qxz, vfma(Qyy, Qyz, Qyz * Qzz));
+    const F2 q2zz = vfma(Qxz, Qxz, vfma(Qyz, Qyz, Qzz * Qzz));
+    const F2 t3 = (1.0f / 3.0f) * trQ2;
+    const F2 cg = vfma(cQ3, trQ2, mk2(cQ, cQ));
+    h[0] = vfma(-cQ2, q2xx - t3, cg * Qxx);
+    h[1] = vfma(-cQ2, q2yy - t3, cg * Qyy);
+    h[2] = vfma(-cQ2, q2zz - t3, cg * Qzz);
+    h[3] = vfma(-cQ2, q2xy, cg * Qxy);
+    h[4] = vfma(-cQ2, q2xz, cg * Qxz);
+    h[5] = vfma(-cQ2, q2yz, cg * Qyz);
+}
+
+// A(c, di, dj, dk) returns an F2 (component c of both cells at that offset; c = 5 is Qzz).
+template <bool kL2, bool kL3, class Acc>
+__device__ __forceinline__ void chem_interior_pair(const Acc& A, const QsrConst& P, const F2 q[5], F2 mu[5],
+                                                   F2 lap[5]) {
+    constexpr bool kMixed = kL2 || kL3;
+    F2 sx[5], sy[5], sz[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        sx[c] = A(c, 1, 0, 0) + A(c, -1, 0, 0);
+        sy[c] = A(c, 0, 1, 0) + A(c, 0, -1, 0);
+        sz[c] = A(c, 0, 0, 1) + A(c, 0, 0, -1);
+        lap[c] = vfma(P.ix2, sx[c], vfma(P.iy2, sy[c], vfma(P.iz2, sz[c], P.lap_c * q[c])));
+    }
+    F2 h[6];
+    bulk_field_pair(q, P.cQ, P.cQ2, P.cQ3, h);
+    h[0] = vfma(-P.Liso, lap[0], h[0]);
+    h[1] = vfma(-P.Liso, lap[3], h[1]);
+    h[2] = vfma(P.Liso, lap[0] + lap[3], h[2]);
+    h[3] = vfma(-P.Liso, lap[1], h[3]);
+    h[4] = vfma(-P.Liso, lap[2], h[4]);
+    h[5] = vfma(-P.Liso, lap[4], h[5]);
+    // undivided mixed second differences (four corners) of the five stored components
+    F2 mxy[5], mxz[5], myz[5];
+    if (kMixed) {
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            mxy[c] = (A(c, 1, 1, 0) - A(c, 1, -1, 0)) - (A(c, -1, 1, 0) - A(c, -1, -1, 0));
+            mxz[c] = (A(c, 1, 0, 1) - A(c, 1, 0, -1)) - (A(c, -1, 0, 1) - A(c, -1, 0, -1));
+            myz[c] = (A(c, 0, 1, 1) - A(c, 0, 1, -1)) - (A(c, 0, -1, 1) - A(c, 0, -1, -1));
+        }
+    }
+    if (kL2) {
+        // d_a D_b = sum_k S_ak(Q_kb) / (4 da dk): wide second differences for k = a, four-corner
+        // ones for k != a (components 0 xx, 1 xy, 2 xz, 3 yy, 4 yz)
+        auto wide = [&](int c, int di, int dj, int dk) {
+            return (A(c, di, dj, dk) + A(c, -di, -dj, -dk)) - 2.0f * q[c];
+        };
+        const F2 wx_xx = wide(0, 2, 0, 0), wx_xy = wide(1, 2, 0, 0), wx_xz = wide(2, 2, 0, 0);
+        const F2 wy_yy = wide(3, 0, 2, 0), wy_xy = wide(1, 0, 2, 0), wy_yz = wide(4, 0, 2, 0);
+        const F2 wz_xx = wide(0, 0, 0, 2), wz_yy = wide(3, 0, 0, 2), wz_xz = wide(2, 0, 0, 2), wz_yz = wide(4, 0, 0, 2);
+        const F2 wz_zz = -(wz_xx + wz_yy);
+        const F2 mxz_zz = -(mxz[0] + mxz[3]), myz_zz = -(myz[0] + myz[3]);
+        const float cxx = P.l2w[0], cyy = P.l2w[1], czz = P.l2w[2], cxy = P.l2w[3], cxz = P.l2w[4], cyz = P.l2w[5];
+        const F2 dxDx = vfma(cxx, wx_xx, vfma(cxy, mxy[1], cxz * mxz[2]));
+        const F2 dyDy = vfma(cxy, mxy[1], vfma(cyy, wy_yy, cyz * myz[4]));
+        const F2 dzDz = vfma(cxz, mxz[2], vfma(cyz, myz[4], czz * wz_zz));
+        const F2 sxy = vfma(cxx, wx_xy, vfma(cxy, mxy[3], vfma(cxz, mxz[4],
+                       vfma(cxy, mxy[0], vfma(cyy, wy_xy, cyz * myz[2])))));
+        const F2 sxz = vfma(cxx, wx_xz, vfma(cxy, mxy[4], vfma(cxz, mxz_zz,
+                       vfma(cxz, mxz[0], vfma(cyz, myz[1], czz * wz_xz)))));
+        const F2 syz = vfma(cxy, mxy[2], vfma(cyy, wy_yz, vfma(cyz, myz_zz,
+                       vfma(cxz, mxz[1], vfma(cyz, myz[3], czz * wz_yz)))));
+        h[0] = h[0] - dxDx;
+        h[1] = h[1] - dyDy;
+        h[2] = h[2] - dzDz;
+        h[3] = h[3] - sxy;
+        h[4] = h[4] - sxz;
+        h[5] = h[5] - syz;
+    }
+    F2 corr = (1.0f / 3.0f) * (h[0] + h[1] + h[2]);
+    mu[0] = h[0] - corr;
+    mu[1] = h[3];
+    mu[2] = h[4];
+    mu[3] = h[1] - corr;
+    mu[4] = h[5];
+    if (kL3) {
+        F2 d[5][3];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            d[c][0] = A(c, 1, 0, 0) - A(c, -1, 0, 0);
+            d[c][1] = A(c, 0, 1, 0) - A(c, 0, -1, 0);
+            d[c][2] = A(c, 0, 0, 1) - A(c, 0, 0, -1);
+        }
+        F2 d5[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) d5[a] = -(d[0][a] + d[3][a]);
+        auto M = [&](int a, int b) {
+            const F2 diag = vfma(d[0][a], d[0][b], vfma(d[3][a], d[3][b], d5[a] * d5[b]));
+            const F2 off = vfma(d[1][a], d[1][b], vfma(d[2][a], d[2][b], d[4][a] * d[4][b]));
+            return vfma(2.0f, off, diag);
+        };
+        F2 hx[6] = {mu[0], mu[3], -(mu[0] + mu[3]), mu[1], mu[2], mu[4]};
+        hx[0] = vfma(P.l3m[0], M(0, 0), hx[0]);
+        hx[1] = vfma(P.l3m[1], M(1, 1), hx[1]);
+        hx[2] = vfma(P.l3m[2], M(2, 2), hx[2]);
+        hx[3] = vfma(P.l3m[3], M(0, 1), hx[3]);
+        hx[4] = vfma(P.l3m[4], M(0, 2), hx[4]);
+        hx[5] = vfma(P.l3m[5], M(1, 2), hx[5]);
+        // centre divergence D_x = d_x Q_xx + d_y Q_xy + d_z Q_xz, ... (QSR.cu:325-371), times 1/(2 da)
+        const F2 Dc0 = P.i2x * vfma(P.i2x, d[0][0], vfma(P.i2y, d[1][1], P.i2z * d[2][2]));
+        const F2 Dc1 = P.i2y * vfma(P.i2x, d[1][0], vfma(P.i2y, d[3][1], P.i2z * d[4][2]));
+        const F2 Dc2 = P.i2z * vfma(P.i2x, d[2][0], vfma(P.i2y, d[4][1], P.i2z * d5[2]));
+        const F2 Qzz = -(q[0] + q[3]);
+        const F2 wxx = P.ix2 * q[0], wyy = P.iy2 * q[3], wzz = P.iz2 * Qzz;
+        const F2 wxy = (2.0f * P.i4xy) * q[1], wxz = (2.0f * P.i4xz) * q[2], wyz = (2.0f * P.i4yz) * q[4];
+        F2 B[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const F2 q2 = 2.0f * q[c];
+            const F2 contract = vfma(wxx, sx[c] - q2, vfma(wyy, sy[c] - q2, vfma(wzz, sz[c] - q2,
+                                vfma(wxy, mxy[c], vfma(wxz, mxz[c], wyz * myz[c])))));
+            B[c] = vfma(Dc0, d[c][0], vfma(Dc1, d[c][1], vfma(Dc2, d[c][2], contract)));
+        }
+        hx[0] = vfma(-P.L3, B[0], hx[0]);
+        hx[1] = vfma(-P.L3, B[3], hx[1]);
+        hx[2] = vfma(P.L3, B[0] + B[3], hx[2]);  // - L3 B_zz, B_zz = -(B_xx + B_yy)
+        hx[3] = vfma(-P.L3, B[1], hx[3]);
+        hx[4] = vfma(-P.L3, B[2], hx[4]);
+        hx[5] = vfma(-P.L3, B[4], hx[5]);
+        corr = (1.0f / 3.0f) * (hx[0] + hx[1] + hx[2]);
+        mu[0] = hx[0] - corr;
+        mu[3] = hx[1] - corr;
+        mu[1] = hx[3];
+        mu[2] = hx[4];
+        mu[4] = hx[5];
+    }
+}
+
 // Explicit update with compensated storage: a cell holds hi + lo (two FP32 words). The
 // increment -(dt/gamma) mu (+ noise) is added to hi exactly (Knuth's TwoSum) and the rounding
 // error carried in lo, so the stored value keeps about 48 significant bits over any number of

@@ -55,8 +55,9 @@ constexpr int LOOK = 2;              // the cells of plane i read planes i-2 .. 
 // runs three CTAs (24 warps) per SM: 7 slots (~67 KB) and at most 80 registers a thread. The
 // L2/L3 steps need more registers (the mixed and wide second differences) and run two CTAs per
 // SM with 9 slots (~86 KB, four planes in flight).
-template <bool kD>
-__host__ __device__ constexpr int nq() { return kD ? 9 : 7; }
+// (two cells per thread: 128-thread CTAs, three per SM, 7 slots)
+template <bool kD, bool kPair = false>
+__host__ __device__ constexpr int nq() { return (kD && !kPair) ? 9 : 7; }
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
 constexpr int CHUNK = 16;            // planes per work item (default; tunable)
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
@@ -142,9 +143,9 @@ struct TileSmem {
     int* s_item;        // work item broadcast (persistent kernel)
 };
 
-template <bool kD>
+template <bool kD, bool kPair = false>
 __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
-    constexpr int NQ = nq<kD>();
+    constexpr int NQ = nq<kD, kPair>();
     TileSmem S;
     S.sq = reinterpret_cast<float*>(raw);
     S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * PLANE);
@@ -153,8 +154,10 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
     S.s_item = S.s_abort + 1;
     return S;
 }
-template <bool kD>
-__host__ __device__ constexpr size_t tile_smem_bytes() { return (size_t)nq<kD>() * PLANE * 4 + nq<kD>() * 8 + nq<kD>() * 4 + 16; }
+template <bool kD, bool kPair = false>
+__host__ __device__ constexpr size_t tile_smem_bytes() {
+    return (size_t)nq<kD, kPair>() * PLANE * 4 + nq<kD, kPair>() * 8 + nq<kD, kPair>() * 4 + 16;
+}
 
 // A warp's arrival on a slot counter: returns the count before it (acquire-release at CTA
 // scope, so the warp's reads of the plane happen before the slot is refilled).
@@ -319,10 +322,209 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     return ok;
 }
 
-template <bool kD>
+// Shared-memory accessor of two cells of one plane: local (jl, kl) and (jl + 4, kl).
+struct SmemQ2 {
+    const float* pl[5];
+    int off;
+    __device__ __forceinline__ F2 operator()(int c, int di, int dj, int dk) const {
+        const float* s = pl[di + 2] + off + dj * RW + dk;
+        if (c < 5) return mk2(s[c * CSTR], s[c * CSTR + 4 * RW]);
+        return mk2(-(s[0] + s[3 * CSTR]), -(s[4 * RW] + s[3 * CSTR + 4 * RW]));
+    }
+};
+constexpr int PAIR_THREADS = TK * TJ / 2;  // 128: each thread updates rows jl and jl + 4 of the tile
+constexpr int PAIR_NWARP = PAIR_THREADS / 32;
+
+// process_tile for 128 threads, two cells per thread (rows w and w + 4 of warp w): the interior
+// chemical potential of both cells runs as one packed (FFMA2 / FADD2 / FMUL2) instruction stream;
+// face cells, the strong-anchoring rewrite and the update run per cell.
+template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
+__device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* __restrict__ qout,
+                                                  const uint8_t* __restrict__ flags, int j0, int k0, int ib, int ie,
+                                                  const QsrConst& P, const TileSmem& S, uint32_t& phase,
+                                                  int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
+                                                  float* __restrict__ lo_out = nullptr) {
+    constexpr int NQ = nq<kL2 || kL3, true>();
+    float* sq = S.sq;
+    uint64_t* bar = S.bar;
+    const int base = ib - 2;
+    const int tid = threadIdx.x;
+    const int kl = tid & 31, w = tid >> 5;
+    auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
+    auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
+    auto issue = [&](int p) {
+        uint64_t* b = &bar[slot(p)];
+        if (p >= 0 && p < P.Nx && p < ie + LOOK) {
+            fence_proxy_async();
+            mbar_expect_tx(b, PLANE_BYTES);
+            tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
+        } else {
+            mbar_arrive(b);
+        }
+    };
+    if (tid == 0)
+        for (int p = base; p < base + NQ; ++p) issue(p);
+    bool ok = true;
+    auto wait_plane = [&](int p) {
+        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
+            atomicExch(err, LDG_ERR_TIMEOUT);
+            *(volatile int*)S.s_abort = 1;
+            ok = false;
+        }
+    };
+    const int issued_end = ie + NQ - 2;
+    constexpr int kLo = kL2 ? 2 : 1;
+    const int k = k0 + kl;
+    int jr[2];
+    bool in_grid[2], jk_int[2];
+    long long cell0[2];
+    uint8_t f_next[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        jr[r] = j0 + w + 4 * r;
+        in_grid[r] = (jr[r] < P.Ny) && (k < P.Nz);
+        jk_int[r] = jr[r] >= kLo && jr[r] <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
+        cell0[r] = (long long)jr[r] * P.sj + k;
+        f_next[r] = in_grid[r] ? __ldg(flags + (long long)ib * P.si + cell0[r]) : 0;
+    }
+    const float* qpl[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+    int waited_end = base;
+    for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
+    waited_end = ib + LOOK;
+    for (int i = ib; i < ie; ++i) {
+        if (*(volatile int*)S.s_abort) { ok = false; break; }
+        uint8_t f[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            f[r] = f_next[r];
+            if (in_grid[r] && i + 1 < ie) f_next[r] = __ldg(flags + (long long)(i + 1) * P.si + cell0[r]);
+        }
+        wait_plane(i + LOOK);
+        waited_end = i + LOOK + 1;
+        if (!ok) break;
+        bool fixed[2], move[2];
+        bool interior = true;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            fixed[r] = in_grid[r] && !kRHS && (f[r] & kFixed);
+            move[r] = in_grid[r] && (f[r] & kMove) != 0;
+            interior = interior && (!move[r] || (jk_int[r] && i >= kLo && i <= P.Nx - 1 - kLo));
+        }
+        const bool warp_interior = __all_sync(0xffffffffu, interior) != 0;
+        const bool any_move = __any_sync(0xffffffffu, move[0] || move[1]) != 0;
+        float mu[2][5], lap[2][5], c[2][5];
+        if (any_move) {
+            SmemQ A[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+#pragma unroll
+                for (int d = 0; d < 5; ++d) A[r].pl[d] = qpl[d];
+                A[r].off = (w + 4 * r + HJ) * RW + (kl + HK);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) c[r][m] = A[r](m, 0, 0, 0);
+            }
+            if (warp_interior) {
+                SmemQ2 A2;
+#pragma unroll
+                for (int d = 0; d < 5; ++d) A2.pl[d] = qpl[d];
+                A2.off = A[0].off;
+                F2 q2[5], mu2[5], lap2[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) q2[m] = mk2(c[0][m], c[1][m]);
+                chem_interior_pair<kL2, kL3>(A2, P, q2, mu2, lap2);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    mu[0][m] = mu2[m].v.x; mu[1][m] = mu2[m].v.y;
+                    lap[0][m] = lap2[m].v.x; lap[1][m] = lap2[m].v.y;
+                }
+                const bool anch0 = move[0] && (f[0] & kAnchor), anch1 = move[1] && (f[1] & kAnchor);
+                if (__any_sync(0xffffffffu, anch0 || anch1)) {
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        if (r == 0 ? anch0 : anch1) {
+                            float Q0[5];
+                            surface_q0(P, i, jr[r], k, Q0);
+#pragma unroll
+                            for (int m = 0; m < 5; ++m) mu[r][m] += P.Weff * (c[r][m] - Q0[m]);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+                    if (move[r]) {
+                        const FlyD<SmemQ> DA{&A[r], &P, i, jr[r], k};
+                        chem_potential<kL2, kL3, true>(A[r], DA, P, i, jr[r], k, c[r], (f[r] & kAnchor) != 0, mu[r],
+                                                       lap[r]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            if (!(fixed[r] || move[r])) continue;
+            const long long id = (long long)i * P.si + cell0[r];
+            float o[5];
+            if (fixed[r]) {
+                surface_q0(P, i, jr[r], k, o);
+                if (kComp) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
+                }
+            } else {
+                const uint32_t cell = (uint32_t)(k + P.Nz * (jr[r] + P.Ny * i));
+                if (kRHS) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) o[m] = c[r][m] - P.mob_dt * mu[r][m] - P.alpha * lap[r][m];
+                    if (kNoise) {
+                        float g[5];
+                        normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
+                    }
+                } else if (kComp) {
+                    float lo[5];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
+                    euler_update_comp(P, c[r], lo, mu[r], cell, kNoise, o);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
+                } else {
+                    euler_update(P, c[r], mu[r], cell, kNoise, o);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
+        }
+        __syncwarp();
+        if (kl == 0) {
+            const uint32_t sl = slot(i - 2);
+            if (arrive_freed(&S.freed[sl]) % (unsigned)PAIR_NWARP == (unsigned)PAIR_NWARP - 1u) issue(i - 2 + NQ);
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
+        qpl[4] = sq + slot(i + 3) * PLANE;
+    }
+    if (ok) {
+        for (int p = waited_end; p < issued_end; ++p) wait_plane(p);
+    } else {
+        for (int p = waited_end; p < issued_end; ++p)
+            if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) break;
+    }
+    const int n_issued = issued_end - base;
+#pragma unroll
+    for (int sl = 0; sl < NQ; ++sl) {
+        const int uses = (n_issued > sl) ? (n_issued - sl + NQ - 1) / NQ : 0;
+        phase ^= (uint32_t)(uses & 1) << sl;
+    }
+    return ok;
+}
+
+template <bool kD, bool kPair = false>
 __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < nq<kD>(); ++s) {
+        for (int s = 0; s < nq<kD, kPair>(); ++s) {
             mbar_init(&S.bar[s], 1);
             S.freed[s] = 0;
         }
@@ -330,6 +532,21 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
         *S.s_abort = 0;
     }
     __syncthreads();
+}
+
+// Single grid, two cells per thread (128 threads): three CTAs per SM.
+template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
+__global__ void __launch_bounds__(PAIR_THREADS, 3)
+    k_step_tiled_pair(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout,
+                      const uint8_t* __restrict__ flags, const int4* __restrict__ items, QsrConst P,
+                      int* __restrict__ err, const float* __restrict__ lo_in, float* __restrict__ lo_out) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const TileSmem S = tile_smem<kL2 || kL3, true>(smem_raw);
+    tile_smem_init<kL2 || kL3, true>(S);
+    const int4 item = items[blockIdx.x];
+    uint32_t phase = 0;
+    process_tile_pair<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase,
+                                                     err, lo_in, lo_out);
 }
 
 // Single grid: one work item per CTA; two CTAs per SM with the L2/L3 terms, three without.
@@ -474,7 +691,7 @@ struct TiledPlan {
     int* err = nullptr;           // device error word
     CUtensorMap tmap[2];
     const float* bufs[2] = {nullptr, nullptr};
-    size_t smem_bytes[2] = {0, 0};  // [L1 only, with L2/L3]
+    size_t smem_bytes[3] = {0, 0, 0};  // [L1 only, with L2/L3, with L2/L3 two cells per thread]
 };
 
 // Work items for chunks of `chunk` planes. In each row band and plane chunk the k tiles start at
@@ -519,6 +736,15 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
     });
     if (active) *active = act;
     return items;
+}
+
+// Two cells per thread for the L2/L3 steps (LDG_QSR_PAIR=0 selects one cell per thread).
+inline bool tiled_pair_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("LDG_QSR_PAIR");
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
 
 inline int tiled_default_chunk() {
@@ -623,6 +849,7 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     plan.bufs[1] = buf1;
     plan.smem_bytes[0] = tile_smem_bytes<false>();
     plan.smem_bytes[1] = tile_smem_bytes<true>();
+    plan.smem_bytes[2] = tile_smem_bytes<true, true>();
     plan.ok = true;
     return LDG_OK;
 }
@@ -639,6 +866,19 @@ inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const ui
         configured = true;
     }
     if (plan.n_items == 0) return LDG_OK;
+    if ((L2 || L3) && tiled_pair_enabled()) {
+        const size_t smem2 = plan.smem_bytes[2];
+        static bool configured_pair = false;
+        if (!configured_pair) {
+            LDG_CUDA(cudaFuncSetAttribute(k_step_tiled_pair<L2, L3, N, R, K>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+            configured_pair = true;
+        }
+        k_step_tiled_pair<L2, L3, N, R, K><<<plan.n_items, PAIR_THREADS, smem2, st>>>(plan.tmap[which], out, flags,
+                                                                                     plan.items, P, plan.err, lo_in,
+                                                                                     lo_out);
+        return LDG_OK;
+    }
     k_step_tiled<L2, L3, N, R, K><<<plan.n_items, THREADS, smem, st>>>(plan.tmap[which], out, flags, plan.items, P,
                                                                        plan.err, lo_in, lo_out);
     return LDG_OK;
