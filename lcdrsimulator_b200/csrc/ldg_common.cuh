@@ -531,78 +531,87 @@ __device__ __forceinline__ void bulk_field_pair(const F2 q[5], float cQ, float c
 }
 
 // A(c, di, dj, dk) returns an F2 (component c of both cells at that offset; c = 5 is Qzz).
+// The terms are formed one stored component at a time (components 0 xx, 1 xy, 2 xz, 3 yy, 4 yz),
+// so that only the first differences of every component stay live for M_ab and the divergence:
+//  * its face neighbours give its Laplacian and first differences;
+//  * its four-corner and wide second differences go straight into the L2 term d_a D_b, which for
+//    an interior cell is sum_k S_ak(Q_kb) / (4 da dk) (wide second difference for k = a, four
+//    corners for k != a), and into its L3 contraction Q_ab d_a d_b Q_c;
+//  * h is projected traceless once at the end (the projection is linear, so projecting after the
+//    L1/L2 terms and again after L3, as QSR.cu:462-469 and 611-619 do, gives the same result).
 template <bool kL2, bool kL3, class Acc>
 __device__ __forceinline__ void chem_interior_pair(const Acc& A, const QsrConst& P, const F2 q[5], F2 mu[5],
                                                    F2 lap[5]) {
-    constexpr bool kMixed = kL2 || kL3;
-    F2 sx[5], sy[5], sz[5];
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-        sx[c] = A(c, 1, 0, 0) + A(c, -1, 0, 0);
-        sy[c] = A(c, 0, 1, 0) + A(c, 0, -1, 0);
-        sz[c] = A(c, 0, 0, 1) + A(c, 0, 0, -1);
-        lap[c] = vfma(P.ix2, sx[c], vfma(P.iy2, sy[c], vfma(P.iz2, sz[c], P.lap_c * q[c])));
-    }
     F2 h[6];
     bulk_field_pair(q, P.cQ, P.cQ2, P.cQ3, h);
-    h[0] = vfma(-P.Liso, lap[0], h[0]);
-    h[1] = vfma(-P.Liso, lap[3], h[1]);
-    h[2] = vfma(P.Liso, lap[0] + lap[3], h[2]);
-    h[3] = vfma(-P.Liso, lap[1], h[3]);
-    h[4] = vfma(-P.Liso, lap[2], h[4]);
-    h[5] = vfma(-P.Liso, lap[4], h[5]);
-    // undivided mixed second differences (four corners) of the five stored components
-    F2 mxy[5], mxz[5], myz[5];
-    if (kMixed) {
+    const float cxx = P.l2w[0], cyy = P.l2w[1], czz = P.l2w[2], cxy = P.l2w[3], cxz = P.l2w[4], cyz = P.l2w[5];
+    // second-derivative weights of the L3 contraction, shared by every component
+    const F2 Qzz = -(q[0] + q[3]);
+    const F2 wxx = P.ix2 * q[0], wyy = P.iy2 * q[3], wzz = P.iz2 * Qzz;
+    const F2 wxy = (2.0f * P.i4xy) * q[1], wxz = (2.0f * P.i4xz) * q[2], wyz = (2.0f * P.i4yz) * q[4];
+    F2 d[5][3], contract[5];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            mxy[c] = (A(c, 1, 1, 0) - A(c, 1, -1, 0)) - (A(c, -1, 1, 0) - A(c, -1, -1, 0));
-            mxz[c] = (A(c, 1, 0, 1) - A(c, 1, 0, -1)) - (A(c, -1, 0, 1) - A(c, -1, 0, -1));
-            myz[c] = (A(c, 0, 1, 1) - A(c, 0, 1, -1)) - (A(c, 0, -1, 1) - A(c, 0, -1, -1));
+    for (int c = 0; c < 5; ++c) {
+        const F2 px = A(c, 1, 0, 0), mx = A(c, -1, 0, 0), py = A(c, 0, 1, 0), my = A(c, 0, -1, 0);
+        const F2 pz = A(c, 0, 0, 1), mz = A(c, 0, 0, -1);
+        const F2 sx = px + mx, sy = py + my, sz = pz + mz;
+        d[c][0] = px - mx;
+        d[c][1] = py - my;
+        d[c][2] = pz - mz;
+        lap[c] = vfma(P.ix2, sx, vfma(P.iy2, sy, vfma(P.iz2, sz, P.lap_c * q[c])));
+        // -Liso lap into h (h_zz takes -Liso lap_zz = Liso (lap_xx + lap_yy))
+        if (c == 0) { h[0] = vfma(-P.Liso, lap[c], h[0]); h[2] = vfma(P.Liso, lap[c], h[2]); }
+        if (c == 3) { h[1] = vfma(-P.Liso, lap[c], h[1]); h[2] = vfma(P.Liso, lap[c], h[2]); }
+        if (c == 1) h[3] = vfma(-P.Liso, lap[c], h[3]);
+        if (c == 2) h[4] = vfma(-P.Liso, lap[c], h[4]);
+        if (c == 4) h[5] = vfma(-P.Liso, lap[c], h[5]);
+        if (kL2 || kL3) {
+            const F2 mxy = (A(c, 1, 1, 0) - A(c, 1, -1, 0)) - (A(c, -1, 1, 0) - A(c, -1, -1, 0));
+            const F2 mxz = (A(c, 1, 0, 1) - A(c, 1, 0, -1)) - (A(c, -1, 0, 1) - A(c, -1, 0, -1));
+            const F2 myz = (A(c, 0, 1, 1) - A(c, 0, 1, -1)) - (A(c, 0, -1, 1) - A(c, 0, -1, -1));
+            if (kL2) {
+                const F2 q2 = 2.0f * q[c];
+                if (c == 0) {  // xx
+                    h[0] = vfma(-cxx, (A(0, 2, 0, 0) + A(0, -2, 0, 0)) - q2, h[0]);
+                    h[2] = vfma(czz, (A(0, 0, 0, 2) + A(0, 0, 0, -2)) - q2, h[2]);
+                    h[3] = vfma(-cxy, mxy, h[3]);
+                    h[5] = vfma(cyz, myz, h[5]);
+                } else if (c == 3) {  // yy
+                    h[1] = vfma(-cyy, (A(3, 0, 2, 0) + A(3, 0, -2, 0)) - q2, h[1]);
+                    h[2] = vfma(czz, (A(3, 0, 0, 2) + A(3, 0, 0, -2)) - q2, h[2]);
+                    h[3] = vfma(-cxy, mxy, h[3]);
+                    h[4] = vfma(cxz, mxz, h[4]);
+                } else if (c == 1) {  // xy
+                    h[0] = vfma(-cxy, mxy, h[0]);
+                    h[1] = vfma(-cxy, mxy, h[1]);
+                    h[3] = vfma(-cxx, (A(1, 2, 0, 0) + A(1, -2, 0, 0)) - q2, h[3]);
+                    h[3] = vfma(-cyy, (A(1, 0, 2, 0) + A(1, 0, -2, 0)) - q2, h[3]);
+                    h[4] = vfma(-cyz, myz, h[4]);
+                    h[5] = vfma(-cxz, mxz, h[5]);
+                } else if (c == 2) {  // xz
+                    h[0] = vfma(-cxz, mxz, h[0]);
+                    h[2] = vfma(-cxz, mxz, h[2]);
+                    h[3] = vfma(-cyz, myz, h[3]);
+                    h[4] = vfma(-cxx, (A(2, 2, 0, 0) + A(2, -2, 0, 0)) - q2, h[4]);
+                    h[4] = vfma(-czz, (A(2, 0, 0, 2) + A(2, 0, 0, -2)) - q2, h[4]);
+                    h[5] = vfma(-cxy, mxy, h[5]);
+                } else {  // yz
+                    h[1] = vfma(-cyz, myz, h[1]);
+                    h[2] = vfma(-cyz, myz, h[2]);
+                    h[3] = vfma(-cxz, mxz, h[3]);
+                    h[4] = vfma(-cxy, mxy, h[4]);
+                    h[5] = vfma(-cyy, (A(4, 0, 2, 0) + A(4, 0, -2, 0)) - q2, h[5]);
+                    h[5] = vfma(-czz, (A(4, 0, 0, 2) + A(4, 0, 0, -2)) - q2, h[5]);
+                }
+            }
+            if (kL3) {
+                const F2 q2 = 2.0f * q[c];
+                contract[c] = vfma(wxx, sx - q2, vfma(wyy, sy - q2, vfma(wzz, sz - q2,
+                              vfma(wxy, mxy, vfma(wxz, mxz, wyz * myz)))));
+            }
         }
     }
-    if (kL2) {
-        // d_a D_b = sum_k S_ak(Q_kb) / (4 da dk): wide second differences for k = a, four-corner
-        // ones for k != a (components 0 xx, 1 xy, 2 xz, 3 yy, 4 yz)
-        auto wide = [&](int c, int di, int dj, int dk) {
-            return (A(c, di, dj, dk) + A(c, -di, -dj, -dk)) - 2.0f * q[c];
-        };
-        const F2 wx_xx = wide(0, 2, 0, 0), wx_xy = wide(1, 2, 0, 0), wx_xz = wide(2, 2, 0, 0);
-        const F2 wy_yy = wide(3, 0, 2, 0), wy_xy = wide(1, 0, 2, 0), wy_yz = wide(4, 0, 2, 0);
-        const F2 wz_xx = wide(0, 0, 0, 2), wz_yy = wide(3, 0, 0, 2), wz_xz = wide(2, 0, 0, 2), wz_yz = wide(4, 0, 0, 2);
-        const F2 wz_zz = -(wz_xx + wz_yy);
-        const F2 mxz_zz = -(mxz[0] + mxz[3]), myz_zz = -(myz[0] + myz[3]);
-        const float cxx = P.l2w[0], cyy = P.l2w[1], czz = P.l2w[2], cxy = P.l2w[3], cxz = P.l2w[4], cyz = P.l2w[5];
-        const F2 dxDx = vfma(cxx, wx_xx, vfma(cxy, mxy[1], cxz * mxz[2]));
-        const F2 dyDy = vfma(cxy, mxy[1], vfma(cyy, wy_yy, cyz * myz[4]));
-        const F2 dzDz = vfma(cxz, mxz[2], vfma(cyz, myz[4], czz * wz_zz));
-        const F2 sxy = vfma(cxx, wx_xy, vfma(cxy, mxy[3], vfma(cxz, mxz[4],
-                       vfma(cxy, mxy[0], vfma(cyy, wy_xy, cyz * myz[2])))));
-        const F2 sxz = vfma(cxx, wx_xz, vfma(cxy, mxy[4], vfma(cxz, mxz_zz,
-                       vfma(cxz, mxz[0], vfma(cyz, myz[1], czz * wz_xz)))));
-        const F2 syz = vfma(cxy, mxy[2], vfma(cyy, wy_yz, vfma(cyz, myz_zz,
-                       vfma(cxz, mxz[1], vfma(cyz, myz[3], czz * wz_yz)))));
-        h[0] = h[0] - dxDx;
-        h[1] = h[1] - dyDy;
-        h[2] = h[2] - dzDz;
-        h[3] = h[3] - sxy;
-        h[4] = h[4] - sxz;
-        h[5] = h[5] - syz;
-    }
-    F2 corr = (1.0f / 3.0f) * (h[0] + h[1] + h[2]);
-    mu[0] = h[0] - corr;
-    mu[1] = h[3];
-    mu[2] = h[4];
-    mu[3] = h[1] - corr;
-    mu[4] = h[5];
     if (kL3) {
-        F2 d[5][3];
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            d[c][0] = A(c, 1, 0, 0) - A(c, -1, 0, 0);
-            d[c][1] = A(c, 0, 1, 0) - A(c, 0, -1, 0);
-            d[c][2] = A(c, 0, 0, 1) - A(c, 0, 0, -1);
-        }
         F2 d5[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) d5[a] = -(d[0][a] + d[3][a]);
@@ -611,41 +620,33 @@ __device__ __forceinline__ void chem_interior_pair(const Acc& A, const QsrConst&
             const F2 off = vfma(d[1][a], d[1][b], vfma(d[2][a], d[2][b], d[4][a] * d[4][b]));
             return vfma(2.0f, off, diag);
         };
-        F2 hx[6] = {mu[0], mu[3], -(mu[0] + mu[3]), mu[1], mu[2], mu[4]};
-        hx[0] = vfma(P.l3m[0], M(0, 0), hx[0]);
-        hx[1] = vfma(P.l3m[1], M(1, 1), hx[1]);
-        hx[2] = vfma(P.l3m[2], M(2, 2), hx[2]);
-        hx[3] = vfma(P.l3m[3], M(0, 1), hx[3]);
-        hx[4] = vfma(P.l3m[4], M(0, 2), hx[4]);
-        hx[5] = vfma(P.l3m[5], M(1, 2), hx[5]);
+        // (L3 / 2) M_ab: h_zz first, as -(hx_xx + hx_yy) of the projected field gets it below
+        h[0] = vfma(P.l3m[0], M(0, 0), h[0]);
+        h[1] = vfma(P.l3m[1], M(1, 1), h[1]);
+        h[2] = vfma(P.l3m[2], M(2, 2), h[2]);
+        h[3] = vfma(P.l3m[3], M(0, 1), h[3]);
+        h[4] = vfma(P.l3m[4], M(0, 2), h[4]);
+        h[5] = vfma(P.l3m[5], M(1, 2), h[5]);
         // centre divergence D_x = d_x Q_xx + d_y Q_xy + d_z Q_xz, ... (QSR.cu:325-371), times 1/(2 da)
         const F2 Dc0 = P.i2x * vfma(P.i2x, d[0][0], vfma(P.i2y, d[1][1], P.i2z * d[2][2]));
         const F2 Dc1 = P.i2y * vfma(P.i2x, d[1][0], vfma(P.i2y, d[3][1], P.i2z * d[4][2]));
         const F2 Dc2 = P.i2z * vfma(P.i2x, d[2][0], vfma(P.i2y, d[4][1], P.i2z * d5[2]));
-        const F2 Qzz = -(q[0] + q[3]);
-        const F2 wxx = P.ix2 * q[0], wyy = P.iy2 * q[3], wzz = P.iz2 * Qzz;
-        const F2 wxy = (2.0f * P.i4xy) * q[1], wxz = (2.0f * P.i4xz) * q[2], wyz = (2.0f * P.i4yz) * q[4];
         F2 B[5];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            const F2 q2 = 2.0f * q[c];
-            const F2 contract = vfma(wxx, sx[c] - q2, vfma(wyy, sy[c] - q2, vfma(wzz, sz[c] - q2,
-                                vfma(wxy, mxy[c], vfma(wxz, mxz[c], wyz * myz[c])))));
-            B[c] = vfma(Dc0, d[c][0], vfma(Dc1, d[c][1], vfma(Dc2, d[c][2], contract)));
-        }
-        hx[0] = vfma(-P.L3, B[0], hx[0]);
-        hx[1] = vfma(-P.L3, B[3], hx[1]);
-        hx[2] = vfma(P.L3, B[0] + B[3], hx[2]);  // - L3 B_zz, B_zz = -(B_xx + B_yy)
-        hx[3] = vfma(-P.L3, B[1], hx[3]);
-        hx[4] = vfma(-P.L3, B[2], hx[4]);
-        hx[5] = vfma(-P.L3, B[4], hx[5]);
-        corr = (1.0f / 3.0f) * (hx[0] + hx[1] + hx[2]);
-        mu[0] = hx[0] - corr;
-        mu[3] = hx[1] - corr;
-        mu[1] = hx[3];
-        mu[2] = hx[4];
-        mu[4] = hx[5];
+        for (int c = 0; c < 5; ++c) B[c] = vfma(Dc0, d[c][0], vfma(Dc1, d[c][1], vfma(Dc2, d[c][2], contract[c])));
+        h[0] = vfma(-P.L3, B[0], h[0]);
+        h[1] = vfma(-P.L3, B[3], h[1]);
+        h[2] = vfma(P.L3, B[0] + B[3], h[2]);  // - L3 B_zz, B_zz = -(B_xx + B_yy)
+        h[3] = vfma(-P.L3, B[1], h[3]);
+        h[4] = vfma(-P.L3, B[2], h[4]);
+        h[5] = vfma(-P.L3, B[4], h[5]);
     }
+    const F2 corr = (1.0f / 3.0f) * (h[0] + h[1] + h[2]);
+    mu[0] = h[0] - corr;
+    mu[1] = h[3];
+    mu[2] = h[4];
+    mu[3] = h[1] - corr;
+    mu[4] = h[5];
 }
 
 // Explicit update with compensated storage: a cell holds hi + lo (two FP32 words). The

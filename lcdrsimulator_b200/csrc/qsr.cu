@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ 
     const int i = item.z;
     const int k = item.y + (int)(threadIdx.x & 31);
     const int j = item.x + (int)(threadIdx.x >> 5);
-    if (k >= P.Nz || j >= P.Ny) return;
+    if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // the first tile of a row may start at k = -2
     const long long id = (long long)i * P.si + (long long)j * P.sj + k;
     const uint8_t f = __ldg(flags + id);
     if (!(f & (kMove | kFixed))) return;

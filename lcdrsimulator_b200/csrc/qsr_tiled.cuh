@@ -45,19 +45,24 @@ constexpr int TK = 32;               // tile width along k (one warp per row)
 constexpr int TJ = 8;                // tile rows along j (one warp each)
 constexpr int THREADS = TK * TJ;
 constexpr int NWARP = THREADS / 32;
-constexpr int HJ = 2, HK = 4;        // halo rows / columns loaded with each plane
-constexpr int RW = TK + 2 * HK;      // 40 floats per smem row
+// Halo rows / columns loaded with each plane: the stencils reach two cells out. The TMA box
+// starts at column k0 - HK, which must be a multiple of 4 floats (16 bytes), so tiles start at
+// k0 = 2 (mod 4) (the first may start at k0 = -2: its two columns outside the grid are zero
+// fill and compute nothing).
+constexpr int HJ = 2, HK = 2;
+constexpr int RW = TK + 2 * HK;      // 36 floats per smem row
 constexpr int ROWS = TJ + 2 * HJ;    // 12 rows
 constexpr int CSTR = RW * ROWS;      // floats per component plane
 constexpr int PLANE = 5 * CSTR;      // floats per plane (all components)
+constexpr int SLOT = (PLANE + 31) / 32 * 32;  // floats per ring slot (TMA destinations 128-byte aligned)
 constexpr int LOOK = 2;              // the cells of plane i read planes i-2 .. i+2
 // Q ring slots: planes i-2 .. i+2 are read at plane i, the rest are in flight. The L1-only step
 // runs three CTAs (24 warps) per SM: 7 slots (~67 KB) and at most 80 registers a thread. The
 // L2/L3 steps need more registers (the mixed and wide second differences) and run two CTAs per
 // SM with 9 slots (~86 KB, four planes in flight).
-// (two cells per thread: 128-thread CTAs, three per SM, 7 slots)
+// (two cells per thread: 128-thread CTAs, four per SM, 6 slots ~ 52 KB)
 template <bool kD, bool kPair = false>
-__host__ __device__ constexpr int nq() { return (kD && !kPair) ? 9 : 7; }
+__host__ __device__ constexpr int nq() { return kPair ? 6 : (kD ? 9 : 7); }
 constexpr uint32_t PLANE_BYTES = PLANE * 4;
 constexpr int CHUNK = 16;            // planes per work item (default; tunable)
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
@@ -148,7 +153,7 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
     constexpr int NQ = nq<kD, kPair>();
     TileSmem S;
     S.sq = reinterpret_cast<float*>(raw);
-    S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * PLANE);
+    S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * SLOT);
     S.freed = reinterpret_cast<unsigned*>(S.bar + NQ);
     S.s_abort = reinterpret_cast<int*>(S.freed + NQ);
     S.s_item = S.s_abort + 1;
@@ -156,7 +161,7 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
 }
 template <bool kD, bool kPair = false>
 __host__ __device__ constexpr size_t tile_smem_bytes() {
-    return (size_t)nq<kD, kPair>() * PLANE * 4 + nq<kD, kPair>() * 8 + nq<kD, kPair>() * 4 + 16;
+    return (size_t)nq<kD, kPair>() * SLOT * 4 + nq<kD, kPair>() * 8 + nq<kD, kPair>() * 4 + 16;
 }
 
 // A warp's arrival on a slot counter: returns the count before it (acquire-release at CTA
@@ -199,7 +204,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         if (p >= 0 && p < P.Nx && p < ie + LOOK) {
             fence_proxy_async();
             mbar_expect_tx(b, PLANE_BYTES);
-            tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
+            tma_load_4d(sq + slot(p) * SLOT, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
             mbar_arrive(b);
         }
@@ -219,7 +224,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     const int issued_end = ie + NQ - 2;
 
     const int j = j0 + jl, k = k0 + kl;
-    const bool in_grid = (j < P.Ny) && (k < P.Nz);
+    const bool in_grid = (j < P.Ny) && (k >= 0) && (k < P.Nz);
     // Interior cells take the Q-only path: every stencil position within the grid away from the
     // faces (the L2 term reaches two cells out: 2 <= pos <= N - 3; otherwise 1 <= pos <= N - 2).
     constexpr int kLo = kL2 ? 2 : 1;
@@ -229,7 +234,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     // Shared-memory planes i-2 .. i+2 of the current step, rolled forward by one plane per step.
     const float* qpl[5];
 #pragma unroll
-    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * SLOT;
     int waited_end = base;
     for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     waited_end = ib + LOOK;
@@ -302,7 +307,7 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
         }
 #pragma unroll
         for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
-        qpl[4] = sq + slot(i + 3) * PLANE;
+        qpl[4] = sq + slot(i + 3) * SLOT;
     }
     // Drain: every load this item issues lands before the slots are reused or released. After
     // an abort some refills are never issued; those waits give up after their bound.
@@ -357,7 +362,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
         if (p >= 0 && p < P.Nx && p < ie + LOOK) {
             fence_proxy_async();
             mbar_expect_tx(b, PLANE_BYTES);
-            tma_load_4d(sq + slot(p) * PLANE, tm, k0 - HK, j0 - HJ, p, 0, b);
+            tma_load_4d(sq + slot(p) * SLOT, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
             mbar_arrive(b);
         }
@@ -382,14 +387,14 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
         jr[r] = j0 + w + 4 * r;
-        in_grid[r] = (jr[r] < P.Ny) && (k < P.Nz);
+        in_grid[r] = (jr[r] < P.Ny) && (k >= 0) && (k < P.Nz);
         jk_int[r] = jr[r] >= kLo && jr[r] <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
         cell0[r] = (long long)jr[r] * P.sj + k;
         f_next[r] = in_grid[r] ? __ldg(flags + (long long)ib * P.si + cell0[r]) : 0;
     }
     const float* qpl[5];
 #pragma unroll
-    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * PLANE;
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * SLOT;
     int waited_end = base;
     for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     waited_end = ib + LOOK;
@@ -504,7 +509,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
         }
 #pragma unroll
         for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
-        qpl[4] = sq + slot(i + 3) * PLANE;
+        qpl[4] = sq + slot(i + 3) * SLOT;
     }
     if (ok) {
         for (int p = waited_end; p < issued_end; ++p) wait_plane(p);
@@ -534,9 +539,9 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
     __syncthreads();
 }
 
-// Single grid, two cells per thread (128 threads): three CTAs per SM.
+// Single grid, two cells per thread (128 threads): four CTAs per SM.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
-__global__ void __launch_bounds__(PAIR_THREADS, 3)
+__global__ void __launch_bounds__(PAIR_THREADS, 4)
     k_step_tiled_pair(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout,
                       const uint8_t* __restrict__ flags, const int4* __restrict__ items, QsrConst P,
                       int* __restrict__ err, const float* __restrict__ lo_in, float* __restrict__ lo_out) {
@@ -714,7 +719,7 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
                     kmax = std::max(kmax, b.kmax[p - b.ib]);
                 }
             if (kmax < 0) continue;
-            for (int k0 = kmin & ~3; k0 <= kmax; k0 += TK) {
+            for (int k0 = ((kmin - 2) & ~3) + 2; k0 <= kmax; k0 += TK) {
                 int first = -1, last = -1;
                 for (int p = ib; p < ie; ++p) {
                     const int lo = b.kmin[p - b.ib], hi = b.kmax[p - b.ib];
@@ -725,7 +730,7 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
                 }
                 if (first < 0) continue;
                 items.push_back(make_int4(b.j0, k0, first, last + 1));
-                act += (long long)b.rows * (std::min(plan.Nz, k0 + TK) - k0) * (last + 1 - first);
+                act += (long long)b.rows * (std::min(plan.Nz, k0 + TK) - std::max(0, k0)) * (last + 1 - first);
             }
         }
     }
