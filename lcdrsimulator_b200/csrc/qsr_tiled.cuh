@@ -146,8 +146,6 @@ struct TileSmem {
     unsigned* freed;    // nq counters of warps done with the slot's plane
     int* s_abort;       // set when a bounded wait gave up
     int* s_item;        // work item broadcast (persistent kernel)
-    int4* s_desc;       // item descriptors of the plane stream (two-cell kernel)
-    int* s_prod;        // producer state of the plane stream (two-cell kernel)
 };
 
 template <bool kD, bool kPair = false>
@@ -155,17 +153,15 @@ __device__ __forceinline__ TileSmem tile_smem(unsigned char* raw) {
     constexpr int NQ = nq<kD, kPair>();
     TileSmem S;
     S.sq = reinterpret_cast<float*>(raw);
-    S.s_desc = reinterpret_cast<int4*>(S.sq + NQ * SLOT);
-    S.bar = reinterpret_cast<uint64_t*>(S.s_desc + 4);
+    S.bar = reinterpret_cast<uint64_t*>(S.sq + NQ * SLOT);
     S.freed = reinterpret_cast<unsigned*>(S.bar + NQ);
     S.s_abort = reinterpret_cast<int*>(S.freed + NQ);
     S.s_item = S.s_abort + 1;
-    S.s_prod = S.s_item + 1;
     return S;
 }
 template <bool kD, bool kPair = false>
 __host__ __device__ constexpr size_t tile_smem_bytes() {
-    return (size_t)nq<kD, kPair>() * SLOT * 4 + 4 * 16 + nq<kD, kPair>() * 8 + nq<kD, kPair>() * 4 + 8 + 8 * 4;
+    return (size_t)nq<kD, kPair>() * SLOT * 4 + nq<kD, kPair>() * 8 + nq<kD, kPair>() * 4 + 16;
 }
 
 // A warp's arrival on a slot counter: returns the count before it (acquire-release at CTA
@@ -344,247 +340,190 @@ struct SmemQ2 {
 constexpr int PAIR_THREADS = TK * TJ / 2;  // 128: each thread updates rows jl and jl + 4 of the tile
 constexpr int PAIR_NWARP = PAIR_THREADS / 32;
 
-// The two-cell CTA (128 threads; rows w and w + 4 of warp w) is persistent and streams planes:
-// the CTA takes work items from a global counter, and its plane ring runs on without a break from
-// one item into the next. Stream position g (g = 0, 1, 2, ...) of the CTA lives in slot g % NQ and
-// completes phase g / NQ of that slot's barrier; item t occupies positions [base_t, base_t + n_t)
-// with n_t = ie - ib + 4 (planes ib - 2 .. ie + 1). The thread that refills a slot (the lane 0
-// of the last warp done with it) is the producer: it fetches the next item when the current
-// one's planes run out, records its descriptor in a small ring, and after the last item marks
-// the end of work with a plain arrive on the next position. A warp reads the descriptor of an
-// item after waiting for the item's first position, so loads of the next item overlap the last
-// planes of the current one and no CTA stalls between items.
-constexpr int QI = 4;  // item descriptors in the ring (at most two are live)
-
-// Producer state in shared memory: [0] items fetched, [1] work exhausted, [2] base position and
-// [3] length of the item being loaded, [4] next position to issue.
-enum { PROD_FETCHED = 0, PROD_END = 1, PROD_BASE = 2, PROD_LEN = 3, PROD_NEXT = 4 };
-
+// process_tile for 128 threads, two cells per thread (rows w and w + 4 of warp w): the interior
+// chemical potential of both cells runs as one packed (FFMA2 / FADD2 / FMUL2) instruction stream;
+// face cells, the strong-anchoring rewrite and the update run per cell.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
-__device__ __forceinline__ void stream_tiles_pair(const CUtensorMap* tm, float* __restrict__ qout,
-                                                  const uint8_t* __restrict__ flags, const int4* __restrict__ items,
-                                                  int n_items, int* __restrict__ ctl, const QsrConst& P,
-                                                  const TileSmem& S, int* __restrict__ err,
-                                                  const float* __restrict__ lo_in, float* __restrict__ lo_out) {
+__device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* __restrict__ qout,
+                                                  const uint8_t* __restrict__ flags, int j0, int k0, int ib, int ie,
+                                                  const QsrConst& P, const TileSmem& S, uint32_t& phase,
+                                                  int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
+                                                  float* __restrict__ lo_out = nullptr) {
     constexpr int NQ = nq<kL2 || kL3, true>();
     float* sq = S.sq;
     uint64_t* bar = S.bar;
-    volatile int* prod = S.s_prod;
+    const int base = ib - 2;
     const int tid = threadIdx.x;
     const int kl = tid & 31, w = tid >> 5;
-    auto slot = [](int g) { return (uint32_t)g % (uint32_t)NQ; };
-    auto parity = [](int g) { return ((uint32_t)g / (uint32_t)NQ) & 1u; };
-
-    // Issues stream position g (one thread at a time, in increasing g: the issuing threads are
-    // ordered through the acquire-release slot counters).
-    auto issue = [&](int g) {
-        if (prod[PROD_END]) return;
-        uint64_t* b = &bar[slot(g)];
-        if (prod[PROD_FETCHED] == 0 || g == prod[PROD_BASE] + prod[PROD_LEN]) {
-            const int it = atomicAdd(ctl, 1);
-            const int t = prod[PROD_FETCHED];
-            if (it < n_items) {
-                const int4 d = items[it];
-                S.s_desc[t % QI] = d;
-                prod[PROD_BASE] = g;
-                prod[PROD_LEN] = d.w - d.z + 4;
-            } else {
-                S.s_desc[t % QI] = make_int4(0, 0, 0, -1);  // end of work
-                prod[PROD_END] = 1;
-            }
-            prod[PROD_FETCHED] = t + 1;
-            prod[PROD_NEXT] = g + 1;
-            if (it >= n_items) {
-                mbar_arrive(b);
-                return;
-            }
-        }
-        prod[PROD_NEXT] = g + 1;
-        const int4 d = S.s_desc[(prod[PROD_FETCHED] - 1) % QI];
-        const int p = d.z - 2 + (g - prod[PROD_BASE]);
-        if (p >= 0 && p < P.Nx) {
+    auto slot = [&](int p) { return (uint32_t)(p - base) % (uint32_t)NQ; };
+    auto parity = [&](int p) { return ((phase >> slot(p)) & 1u) ^ (((uint32_t)(p - base) / (uint32_t)NQ) & 1u); };
+    auto issue = [&](int p) {
+        uint64_t* b = &bar[slot(p)];
+        if (p >= 0 && p < P.Nx && p < ie + LOOK) {
             fence_proxy_async();
             mbar_expect_tx(b, PLANE_BYTES);
-            tma_load_4d(sq + slot(g) * SLOT, tm, d.y - HK, d.x - HJ, p, 0, b);
+            tma_load_4d(sq + slot(p) * SLOT, tm, k0 - HK, j0 - HJ, p, 0, b);
         } else {
             mbar_arrive(b);
         }
     };
     if (tid == 0)
-        for (int g = 0; g < NQ; ++g) issue(g);
-    __syncthreads();
-
+        for (int p = base; p < base + NQ; ++p) issue(p);
     bool ok = true;
-    // The outcome is made warp-uniform, so a warp leaves its loops together.
-    auto wait_pos = [&](int g) {
-        const bool got = mbar_wait_bounded(&bar[slot(g)], parity(g));
-        if (!__all_sync(0xffffffffu, got)) {
-            if (kl == 0) {
-                atomicExch(err, LDG_ERR_TIMEOUT);
-                *(volatile int*)S.s_abort = 1;
-            }
+    auto wait_plane = [&](int p) {
+        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
+            atomicExch(err, LDG_ERR_TIMEOUT);
+            *(volatile int*)S.s_abort = 1;
             ok = false;
         }
     };
-    // This warp is done with position g: the last warp to arrive refills its slot with g + NQ.
-    auto release = [&](int g) {
-        __syncwarp();
-        if (kl == 0 && arrive_freed(&S.freed[slot(g)]) % (unsigned)PAIR_NWARP == (unsigned)PAIR_NWARP - 1u)
-            issue(g + NQ);
-    };
+    const int issued_end = ie + NQ - 2;
     constexpr int kLo = kL2 ? 2 : 1;
-    int t = 0, gb = 0;
-    while (ok) {
-        wait_pos(gb);
-        if (!ok) break;
-        const int4 d = S.s_desc[t % QI];
-        if (d.w < 0) break;  // end of work
-        const int j0 = d.x, k0 = d.y, ib = d.z, ie = d.w;
-        const int k = k0 + kl;
-        int jr[2];
-        bool in_grid[2], jk_int[2];
-        long long cell0[2];
-        uint8_t f_next[2];
+    const int k = k0 + kl;
+    int jr[2];
+    bool in_grid[2], jk_int[2];
+    long long cell0[2];
+    uint8_t f_next[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        jr[r] = j0 + w + 4 * r;
+        in_grid[r] = (jr[r] < P.Ny) && (k >= 0) && (k < P.Nz);
+        jk_int[r] = jr[r] >= kLo && jr[r] <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
+        cell0[r] = (long long)jr[r] * P.sj + k;
+        f_next[r] = in_grid[r] ? __ldg(flags + (long long)ib * P.si + cell0[r]) : 0;
+    }
+    const float* qpl[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) qpl[d] = sq + slot(ib + d - 2) * SLOT;
+    int waited_end = base;
+    for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
+    waited_end = ib + LOOK;
+    for (int i = ib; i < ie; ++i) {
+        if (*(volatile int*)S.s_abort) { ok = false; break; }
+        uint8_t f[2];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            jr[r] = j0 + w + 4 * r;
-            in_grid[r] = (jr[r] < P.Ny) && (k >= 0) && (k < P.Nz);
-            jk_int[r] = jr[r] >= kLo && jr[r] <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
-            cell0[r] = (long long)jr[r] * P.sj + k;
-            f_next[r] = in_grid[r] ? __ldg(flags + (long long)ib * P.si + cell0[r]) : 0;
+            f[r] = f_next[r];
+            if (in_grid[r] && i + 1 < ie) f_next[r] = __ldg(flags + (long long)(i + 1) * P.si + cell0[r]);
         }
-        // Planes ib - 2 .. ib + 2 of the first computed plane sit at positions gb .. gb + 4; plane
-        // i sits at gb + i - ib + 2.
-        const float* qpl[5];
-#pragma unroll
-        for (int dd = 0; dd < 5; ++dd) qpl[dd] = sq + slot(gb + dd) * SLOT;
-        for (int g = gb + 1; g < gb + 4 && ok; ++g) wait_pos(g);
-        for (int i = ib; i < ie && ok; ++i) {
-            if (*(volatile int*)S.s_abort) { ok = false; break; }
-            uint8_t f[2];
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                f[r] = f_next[r];
-                if (in_grid[r] && i + 1 < ie) f_next[r] = __ldg(flags + (long long)(i + 1) * P.si + cell0[r]);
-            }
-            const int gi = gb + (i - ib) + 2;  // position of plane i
-            wait_pos(gi + LOOK);
-            if (!ok) break;
-            bool fixed[2], move[2];
-            bool interior = true;
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                fixed[r] = in_grid[r] && !kRHS && (f[r] & kFixed);
-                move[r] = in_grid[r] && (f[r] & kMove) != 0;
-                interior = interior && (!move[r] || (jk_int[r] && i >= kLo && i <= P.Nx - 1 - kLo));
-            }
-            const bool warp_interior = __all_sync(0xffffffffu, interior) != 0;
-            const bool any_move = __any_sync(0xffffffffu, move[0] || move[1]) != 0;
-            float mu[2][5], lap[2][5], c[2][5];
-            if (any_move) {
-                SmemQ A[2];
-#pragma unroll
-                for (int r = 0; r < 2; ++r) {
-#pragma unroll
-                    for (int dd = 0; dd < 5; ++dd) A[r].pl[dd] = qpl[dd];
-                    A[r].off = (w + 4 * r + HJ) * RW + (kl + HK);
-#pragma unroll
-                    for (int m = 0; m < 5; ++m) c[r][m] = A[r](m, 0, 0, 0);
-                }
-                if (warp_interior) {
-                    SmemQ2 A2;
-#pragma unroll
-                    for (int dd = 0; dd < 5; ++dd) A2.pl[dd] = qpl[dd];
-                    A2.off = A[0].off;
-                    F2 q2[5], mu2[5], lap2[5];
-#pragma unroll
-                    for (int m = 0; m < 5; ++m) q2[m] = mk2(c[0][m], c[1][m]);
-                    chem_interior_pair<kL2, kL3>(A2, P, q2, mu2, lap2);
-#pragma unroll
-                    for (int m = 0; m < 5; ++m) {
-                        mu[0][m] = mu2[m].v.x; mu[1][m] = mu2[m].v.y;
-                        lap[0][m] = lap2[m].v.x; lap[1][m] = lap2[m].v.y;
-                    }
-                    const bool anch0 = move[0] && (f[0] & kAnchor), anch1 = move[1] && (f[1] & kAnchor);
-                    if (__any_sync(0xffffffffu, anch0 || anch1)) {
-#pragma unroll
-                        for (int r = 0; r < 2; ++r) {
-                            if (r == 0 ? anch0 : anch1) {
-                                float Q0[5];
-                                surface_q0(P, i, jr[r], k, Q0);
-#pragma unroll
-                                for (int m = 0; m < 5; ++m) mu[r][m] += P.Weff * (c[r][m] - Q0[m]);
-                            }
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < 2; ++r)
-                        if (move[r]) {
-                            const FlyD<SmemQ> DA{&A[r], &P, i, jr[r], k};
-                            chem_potential<kL2, kL3, true>(A[r], DA, P, i, jr[r], k, c[r], (f[r] & kAnchor) != 0,
-                                                           mu[r], lap[r]);
-                        }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                if (!(fixed[r] || move[r])) continue;
-                const long long id = (long long)i * P.si + cell0[r];
-                float o[5];
-                if (fixed[r]) {
-                    surface_q0(P, i, jr[r], k, o);
-                    if (kComp) {
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
-                    }
-                } else {
-                    const uint32_t cell = (uint32_t)(k + P.Nz * (jr[r] + P.Ny * i));
-                    if (kRHS) {
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) o[m] = c[r][m] - P.mob_dt * mu[r][m] - P.alpha * lap[r][m];
-                        if (kNoise) {
-                            float g5[5];
-                            normals5(cell, P.instance, P.step, P.key0, P.key1, g5);
-#pragma unroll
-                            for (int m = 0; m < 5; ++m) o[m] += P.sigma * g5[m];
-                        }
-                    } else if (kComp) {
-                        float lo[5];
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
-                        euler_update_comp(P, c[r], lo, mu[r], cell, kNoise, o);
-#pragma unroll
-                        for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
-                    } else {
-                        euler_update(P, c[r], mu[r], cell, kNoise, o);
-                    }
-                }
-#pragma unroll
-                for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
-            }
-            release(gi - LOOK);  // plane i - 2
-#pragma unroll
-            for (int dd = 0; dd < 4; ++dd) qpl[dd] = qpl[dd + 1];
-            qpl[4] = sq + slot(gi + LOOK + 1) * SLOT;
-        }
+        wait_plane(i + LOOK);
+        waited_end = i + LOOK + 1;
         if (!ok) break;
-        // Planes ie - 2 .. ie + 1 (the item's last four positions) are done too.
-        const int n = ie - ib + 4;
-        for (int g = gb + n - 4; g < gb + n; ++g) release(g);
-        gb += n;
-        ++t;
-    }
-    // Every load in flight lands before the CTA exits: after the last warp stops issuing, wait
-    // for the last phase armed on every slot (bounded; a no-op after a normal end of work).
-    __syncthreads();
-    if (tid == 0) {
-        const int issued = prod[PROD_NEXT];
-        for (int s = 0; s < NQ && s < issued; ++s) {
-            const int g = s + (issued - 1 - s) / NQ * NQ;  // the last position issued into slot s
-            if (!mbar_wait_bounded(&bar[s], parity(g))) break;
+        bool fixed[2], move[2];
+        bool interior = true;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            fixed[r] = in_grid[r] && !kRHS && (f[r] & kFixed);
+            move[r] = in_grid[r] && (f[r] & kMove) != 0;
+            interior = interior && (!move[r] || (jk_int[r] && i >= kLo && i <= P.Nx - 1 - kLo));
         }
+        const bool warp_interior = __all_sync(0xffffffffu, interior) != 0;
+        const bool any_move = __any_sync(0xffffffffu, move[0] || move[1]) != 0;
+        float mu[2][5], lap[2][5], c[2][5];
+        if (any_move) {
+            SmemQ A[2];
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+#pragma unroll
+                for (int d = 0; d < 5; ++d) A[r].pl[d] = qpl[d];
+                A[r].off = (w + 4 * r + HJ) * RW + (kl + HK);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) c[r][m] = A[r](m, 0, 0, 0);
+            }
+            if (warp_interior) {
+                SmemQ2 A2;
+#pragma unroll
+                for (int d = 0; d < 5; ++d) A2.pl[d] = qpl[d];
+                A2.off = A[0].off;
+                F2 q2[5], mu2[5], lap2[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) q2[m] = mk2(c[0][m], c[1][m]);
+                chem_interior_pair<kL2, kL3>(A2, P, q2, mu2, lap2);
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    mu[0][m] = mu2[m].v.x; mu[1][m] = mu2[m].v.y;
+                    lap[0][m] = lap2[m].v.x; lap[1][m] = lap2[m].v.y;
+                }
+                const bool anch0 = move[0] && (f[0] & kAnchor), anch1 = move[1] && (f[1] & kAnchor);
+                if (__any_sync(0xffffffffu, anch0 || anch1)) {
+#pragma unroll
+                    for (int r = 0; r < 2; ++r) {
+                        if (r == 0 ? anch0 : anch1) {
+                            float Q0[5];
+                            surface_q0(P, i, jr[r], k, Q0);
+#pragma unroll
+                            for (int m = 0; m < 5; ++m) mu[r][m] += P.Weff * (c[r][m] - Q0[m]);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < 2; ++r)
+                    if (move[r]) {
+                        const FlyD<SmemQ> DA{&A[r], &P, i, jr[r], k};
+                        chem_potential<kL2, kL3, true>(A[r], DA, P, i, jr[r], k, c[r], (f[r] & kAnchor) != 0, mu[r],
+                                                       lap[r]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            if (!(fixed[r] || move[r])) continue;
+            const long long id = (long long)i * P.si + cell0[r];
+            float o[5];
+            if (fixed[r]) {
+                surface_q0(P, i, jr[r], k, o);
+                if (kComp) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = 0.0f;
+                }
+            } else {
+                const uint32_t cell = (uint32_t)(k + P.Nz * (jr[r] + P.Ny * i));
+                if (kRHS) {
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) o[m] = c[r][m] - P.mob_dt * mu[r][m] - P.alpha * lap[r][m];
+                    if (kNoise) {
+                        float g[5];
+                        normals5(cell, P.instance, P.step, P.key0, P.key1, g);
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) o[m] += P.sigma * g[m];
+                    }
+                } else if (kComp) {
+                    float lo[5];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo[m] = __ldg(lo_in + m * P.sc + id);
+                    euler_update_comp(P, c[r], lo, mu[r], cell, kNoise, o);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) lo_out[m * P.sc + id] = lo[m];
+                } else {
+                    euler_update(P, c[r], mu[r], cell, kNoise, o);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) qout[m * P.sc + id] = o[m];
+        }
+        __syncwarp();
+        if (kl == 0) {
+            const uint32_t sl = slot(i - 2);
+            if (arrive_freed(&S.freed[sl]) % (unsigned)PAIR_NWARP == (unsigned)PAIR_NWARP - 1u) issue(i - 2 + NQ);
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
+        qpl[4] = sq + slot(i + 3) * SLOT;
     }
+    if (ok) {
+        for (int p = waited_end; p < issued_end; ++p) wait_plane(p);
+    } else {
+        for (int p = waited_end; p < issued_end; ++p)
+            if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) break;
+    }
+    const int n_issued = issued_end - base;
+#pragma unroll
+    for (int sl = 0; sl < NQ; ++sl) {
+        const int uses = (n_issued > sl) ? (n_issued - sl + NQ - 1) / NQ : 0;
+        phase ^= (uint32_t)(uses & 1) << sl;
+    }
+    return ok;
 }
 
 template <bool kD, bool kPair = false>
@@ -596,32 +535,23 @@ __device__ __forceinline__ void tile_smem_init(const TileSmem& S) {
         }
         mbar_fence_init();
         *S.s_abort = 0;
-        for (int m = 0; m < 8; ++m) S.s_prod[m] = 0;
     }
     __syncthreads();
 }
 
-// Persistent, two cells per thread (128 threads): four CTAs per SM take the work items from
-// ctl[0]; the last CTA to finish resets ctl[0] and ctl[1] (its finish counter) for the next step.
+// Single grid, two cells per thread (128 threads): four CTAs per SM.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
 __global__ void __launch_bounds__(PAIR_THREADS, 4)
     k_step_tiled_pair(const __grid_constant__ CUtensorMap tm_in, float* __restrict__ qout,
-                      const uint8_t* __restrict__ flags, const int4* __restrict__ items, int n_items,
-                      int* __restrict__ ctl, QsrConst P, int* __restrict__ err, const float* __restrict__ lo_in,
-                      float* __restrict__ lo_out) {
+                      const uint8_t* __restrict__ flags, const int4* __restrict__ items, QsrConst P,
+                      int* __restrict__ err, const float* __restrict__ lo_in, float* __restrict__ lo_out) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const TileSmem S = tile_smem<kL2 || kL3, true>(smem_raw);
     tile_smem_init<kL2 || kL3, true>(S);
-    stream_tiles_pair<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, items, n_items, ctl, P, S, err, lo_in,
-                                                     lo_out);
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(reinterpret_cast<unsigned*>(ctl + 1), 1u) == gridDim.x - 1) {
-            ctl[0] = 0;
-            ctl[1] = 0;
-            __threadfence();
-        }
-    }
+    const int4 item = items[blockIdx.x];
+    uint32_t phase = 0;
+    process_tile_pair<kL2, kL3, kNoise, kRHS, kComp>(&tm_in, qout, flags, item.x, item.y, item.z, item.w, P, S, phase,
+                                                     err, lo_in, lo_out);
 }
 
 // Single grid: one work item per CTA; two CTAs per SM with the L2/L3 terms, three without.
@@ -764,7 +694,6 @@ struct TiledPlan {
     int Nz = 0;
     std::vector<TiledBand> bands; // host: the changing cells' extent per row band and plane
     int* err = nullptr;           // device error word
-    int* ctl = nullptr;           // device work counter and finish counter of the persistent kernel
     CUtensorMap tmap[2];
     const float* bufs[2] = {nullptr, nullptr};
     size_t smem_bytes[3] = {0, 0, 0};  // [L1 only, with L2/L3, with L2/L3 two cells per thread]
@@ -917,8 +846,6 @@ inline int tiled_plan_build(TiledPlan& plan, int Nx, int Ny, int Nz, int sj, lon
     if (rc) return rc;
     LDG_CUDA(cudaMalloc(&plan.err, sizeof(int)));
     LDG_CUDA(cudaMemset(plan.err, 0, sizeof(int)));
-    LDG_CUDA(cudaMalloc(&plan.ctl, 2 * sizeof(int)));
-    LDG_CUDA(cudaMemset(plan.ctl, 0, 2 * sizeof(int)));
     rc = tiled_encode(&plan.tmap[0], buf0, Nx, Ny, Nz, sj, si, sc);
     if (rc) return rc;
     rc = tiled_encode(&plan.tmap[1], buf1, Nx, Ny, Nz, sj, si, sc);
@@ -946,20 +873,15 @@ inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const ui
     if (plan.n_items == 0) return LDG_OK;
     if ((L2 || L3) && tiled_pair_enabled()) {
         const size_t smem2 = plan.smem_bytes[2];
-        static int resident = 0;  // CTAs of the persistent grid (SMs x CTAs per SM)
-        if (resident == 0) {
+        static bool configured_pair = false;
+        if (!configured_pair) {
             LDG_CUDA(cudaFuncSetAttribute(k_step_tiled_pair<L2, L3, N, R, K>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-            int dev = 0, sms = 0, per_sm = 0;
-            LDG_CUDA(cudaGetDevice(&dev));
-            LDG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            LDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_tiled_pair<L2, L3, N, R, K>,
-                                                                   PAIR_THREADS, smem2));
-            resident = std::max(1, sms * per_sm);
+            configured_pair = true;
         }
-        const int grid = std::min(plan.n_items, resident);
-        k_step_tiled_pair<L2, L3, N, R, K><<<grid, PAIR_THREADS, smem2, st>>>(
-            plan.tmap[which], out, flags, plan.items, plan.n_items, plan.ctl, P, plan.err, lo_in, lo_out);
+        k_step_tiled_pair<L2, L3, N, R, K><<<plan.n_items, PAIR_THREADS, smem2, st>>>(plan.tmap[which], out, flags,
+                                                                                     plan.items, P, plan.err, lo_in,
+                                                                                     lo_out);
         return LDG_OK;
     }
     k_step_tiled<L2, L3, N, R, K><<<plan.n_items, THREADS, smem, st>>>(plan.tmap[which], out, flags, plan.items, P,
@@ -1013,7 +935,6 @@ inline void tiled_plan_free(TiledPlan& plan) {
     if (plan.items) cudaFree(plan.items);
     if (plan.plane_items) cudaFree(plan.plane_items);
     cudaFree(plan.err);
-    cudaFree(plan.ctl);
     plan = TiledPlan{};
 }
 
