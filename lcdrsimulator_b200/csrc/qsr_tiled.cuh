@@ -350,6 +350,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
                                                   int* __restrict__ err, const float* __restrict__ lo_in = nullptr,
                                                   float* __restrict__ lo_out = nullptr) {
     constexpr int NQ = nq<kL2 || kL3, true>();
+    static_assert(NQ > 2 * LOOK && LOOK == 2, "the ring holds planes i - 2 .. i + 2 and at least one in flight");
     float* sq = S.sq;
     uint64_t* bar = S.bar;
     const int base = ib - 2;
@@ -370,13 +371,18 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
     if (tid == 0)
         for (int p = base; p < base + NQ; ++p) issue(p);
     bool ok = true;
-    auto wait_plane = [&](int p) {
-        if (!mbar_wait_bounded(&bar[slot(p)], parity(p))) {
+    // Waits run in increasing plane order, so each slot's expected parity is tracked by toggling
+    // its bit of `par` after every wait on it (no division per plane).
+    uint32_t par = phase;
+    auto wait_slot = [&](uint32_t sl) {
+        if (!mbar_wait_bounded(&bar[sl], (par >> sl) & 1u)) {
             atomicExch(err, LDG_ERR_TIMEOUT);
             *(volatile int*)S.s_abort = 1;
             ok = false;
         }
+        par ^= 1u << sl;
     };
+    auto wait_plane = [&](int p) { wait_slot(slot(p)); };
     const int issued_end = ie + NQ - 2;
     constexpr int kLo = kL2 ? 2 : 1;
     const int k = k0 + kl;
@@ -398,6 +404,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
     int waited_end = base;
     for (int p = base; p <= ib + LOOK - 1; ++p) wait_plane(p);
     waited_end = ib + LOOK;
+    uint32_t s_w = slot(ib + LOOK);  // slot of plane i + LOOK, advanced by one per plane
     for (int i = ib; i < ie; ++i) {
         if (*(volatile int*)S.s_abort) { ok = false; break; }
         uint8_t f[2];
@@ -406,7 +413,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
             f[r] = f_next[r];
             if (in_grid[r] && i + 1 < ie) f_next[r] = __ldg(flags + (long long)(i + 1) * P.si + cell0[r]);
         }
-        wait_plane(i + LOOK);
+        wait_slot(s_w);
         waited_end = i + LOOK + 1;
         if (!ok) break;
         bool fixed[2], move[2];
@@ -504,12 +511,14 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
         }
         __syncwarp();
         if (kl == 0) {
-            const uint32_t sl = slot(i - 2);
+            // slot of plane i - 2 = slot of plane i + 2 minus four
+            const uint32_t sl = s_w + (NQ - 4) >= (uint32_t)NQ ? s_w - 4 : s_w + (NQ - 4);
             if (arrive_freed(&S.freed[sl]) % (unsigned)PAIR_NWARP == (unsigned)PAIR_NWARP - 1u) issue(i - 2 + NQ);
         }
+        s_w = (s_w + 1 == (uint32_t)NQ) ? 0u : s_w + 1;  // now the slot of plane i + 3
 #pragma unroll
         for (int d = 0; d < 4; ++d) qpl[d] = qpl[d + 1];
-        qpl[4] = sq + slot(i + 3) * SLOT;
+        qpl[4] = sq + s_w * SLOT;
     }
     if (ok) {
         for (int p = waited_end; p < issued_end; ++p) wait_plane(p);
@@ -625,13 +634,14 @@ __host__ __device__ __forceinline__ double ens_S_eq(double A, double B, double C
     return best_S;
 }
 
-template <bool kL2, bool kL3, bool kNoise>
-__global__ void __launch_bounds__(THREADS, (kL2 || kL3) ? 2 : 3)
+// kPair: the two-cell routine (128 threads, four CTAs per SM), else one cell per thread.
+template <bool kL2, bool kL3, bool kNoise, bool kPair>
+__global__ void __launch_bounds__(kPair ? PAIR_THREADS : THREADS, kPair ? 4 : ((kL2 || kL3) ? 2 : 3))
     k_step_ensemble(const CUtensorMap* __restrict__ tms, const EnsInstDev* __restrict__ inst,
                     const EnsItem* __restrict__ items, int n_items, EnsCtl* __restrict__ ctl, int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    const TileSmem S = tile_smem<kL2 || kL3>(smem_raw);
-    tile_smem_init<kL2 || kL3>(S);
+    const TileSmem S = tile_smem<kL2 || kL3, kPair>(smem_raw);
+    tile_smem_init<kL2 || kL3, kPair>(S);
     // Every CTA reads the step index before any CTA of this launch finishes (the last CTA to
     // finish advances it).
     const long long step = *((volatile long long*)&ctl->step);
@@ -658,8 +668,12 @@ __global__ void __launch_bounds__(THREADS, (kL2 || kL3) ? 2 : 3)
             P.S_shell = (float)D.S_custom;
         }
         P.step = step;
-        process_tile<kL2, kL3, kNoise, false>(tms + 2 * e.inst + which, D.q[1 - which], D.flags, e.j0, e.k0, e.ib, e.ie,
-                                              P, S, phase, err);
+        if constexpr (kPair)
+            process_tile_pair<kL2, kL3, kNoise, false>(tms + 2 * e.inst + which, D.q[1 - which], D.flags, e.j0, e.k0,
+                                                       e.ib, e.ie, P, S, phase, err);
+        else
+            process_tile<kL2, kL3, kNoise, false>(tms + 2 * e.inst + which, D.q[1 - which], D.flags, e.j0, e.k0, e.ib,
+                                                  e.ie, P, S, phase, err);
     }
     if (threadIdx.x == 0) {
         __threadfence();
