@@ -204,61 +204,6 @@ __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ 
     for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
 }
 
-// The same sweep with one block (32 x 8) per work item marching along i: each thread keeps the
-// five components of its cell at planes i - 1, i and i + 1 in registers, so the block reads each
-// of its planes from global memory once; the j and k neighbours are the rows the block's warps
-// load (L1) plus one halo row on either side.
-template <bool kLast>
-__global__ void __launch_bounds__(256) k_jacobi_march(const float* __restrict__ rhs, const float* __restrict__ qo,
-                                                      float* __restrict__ qn, const uint8_t* __restrict__ flags,
-                                                      const int4* __restrict__ items, QsrConst P) {
-    const int4 item = items[blockIdx.x];
-    const int k = item.y + (int)(threadIdx.x & 31);
-    const int j = item.x + (int)(threadIdx.x >> 5);
-    if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // no block barrier follows
-    const long long cell0 = (long long)j * P.sj + k;
-    const bool jk_face = (j == 0 || k == 0 || j == P.Ny - 1 || k == P.Nz - 1);
-    const int ib = item.z, ie = item.w;
-    float qm[5], qc[5], qp[5];
-#pragma unroll
-    for (int m = 0; m < 5; ++m) {
-        const float* b = qo + m * P.sc + (long long)ib * P.si + cell0;
-        qc[m] = __ldg(b);
-        qm[m] = ib > 0 ? __ldg(b - P.si) : 0.0f;
-    }
-    for (int i = ib; i < ie; ++i) {
-        const long long id = (long long)i * P.si + cell0;
-        const bool has_next = i + 1 < P.Nx;
-#pragma unroll
-        for (int m = 0; m < 5; ++m) qp[m] = has_next ? __ldg(qo + m * P.sc + id + P.si) : 0.0f;
-        const uint8_t f = __ldg(flags + id);
-        if (f & (kMove | kFixed)) {
-            float o[5];
-            if (kLast && (f & kFixed)) {
-                surface_q0(P, i, j, k, o);
-            } else if (jk_face || i == 0 || i == P.Nx - 1 || !(f & kMove)) {
-#pragma unroll
-                for (int m = 0; m < 5; ++m) o[m] = qc[m];
-            } else {
-#pragma unroll
-                for (int m = 0; m < 5; ++m) {
-                    const float* b = qo + m * P.sc + id;
-                    const float s = P.ix2 * (qp[m] + qm[m]) + P.iy2 * (__ldg(b + P.sj) + __ldg(b - P.sj)) +
-                                    P.iz2 * (__ldg(b + 1) + __ldg(b - 1));
-                    o[m] = (__ldg(rhs + m * P.sc + id) + P.alpha * s) * P.jdenom_inv;
-                }
-            }
-#pragma unroll
-            for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
-        }
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-            qm[m] = qc[m];
-            qc[m] = qp[m];
-        }
-    }
-}
-
 // Host AoS FP64 (reference cell order) <-> device FP32 SoA.
 __global__ void k_aos_to_soa(const double* __restrict__ aos, float* __restrict__ a, float* __restrict__ b,
                              int Nx, int Ny, int Nz, int sj, long long si, long long sc, float* __restrict__ la = nullptr,
@@ -1146,21 +1091,7 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             int c = h->cur;
             for (int it = 0; it < a->jacobi_iters; ++it) {
                 const bool last = (it == a->jacobi_iters - 1);
-                static const bool march = [] {
-                    const char* e = getenv("LDG_JACOBI_MARCH");
-                    return !(e && e[0] == '0');
-                }();
-                if (tiled && march) {
-                    if (h->tiled.n_items > 0) {
-                        const int nb = h->tiled.n_items;
-                        if (last)
-                            k_jacobi_march<true><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                            h->tiled.items, P);
-                        else
-                            k_jacobi_march<false><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                             h->tiled.items, P);
-                    }
-                } else if (tiled) {
+                if (tiled) {
                     if (h->tiled.n_plane_items > 0) {
                         const int nb = h->tiled.n_plane_items;
                         if (last)
