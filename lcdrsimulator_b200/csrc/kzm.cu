@@ -307,6 +307,126 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_async(const float* __rest
     cp_async_wait<0>();  // no copy into this CTA's shared memory outlives it
 }
 
+// Two sites per thread: the same tile, ring, copies and plane loop as k_kzm_step_async with
+// 128 threads, thread (tx, ty) updating rows ty and ty + 4 of the (32 x 8) tile. The Laplacian,
+// bulk field and update of both sites run as one packed FP32 instruction stream (FFMA2 / FADD2 /
+// FMUL2: per site the same fused operations as the one-site kernel); the noise draw, the cap and
+// the stores stay per site.
+constexpr int KPT = KTX * KTY / 2;
+template <bool kNoise>
+__global__ void __launch_bounds__(KPT) k_kzm_step_pair(const float* __restrict__ q, float* __restrict__ out,
+                                                       KzmConst P) {
+    extern __shared__ __align__(16) float ring[];  // [KRING][5][KTY+2][KTX+2]
+    constexpr int ROW = KTX + 2;
+    const int tid = threadIdx.x;
+    const int tx = tid & 31, ty = tid >> 5;
+    const int x0 = blockIdx.x * KTX, y0 = blockIdx.y * KTY, z0 = blockIdx.z * KZC;
+    const int z1 = min(z0 + KZC, P.Nz);
+    const int xr = x0 + tx;
+    const int x = xr % P.Nx;
+    bool valid[2];
+    long long g_c[2];
+    uint32_t cell_base[2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int yr = y0 + ty + 4 * r;
+        valid[r] = (xr < P.Nx) && (yr < P.Ny);
+        const int y = yr % P.Ny;
+        g_c[r] = (long long)y * P.sy + x;
+        cell_base[r] = (uint32_t)(x + P.Nx * y);
+    }
+    const int s_c = (ty + 1) * ROW + tx + 1;  // row ty; row ty + 4 is 4 * ROW further
+    constexpr int NE = 5 * KPS;
+    constexpr int PER = (NE + KPT - 1) / KPT;
+    long long goff[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int e = tid + t * KPT;
+        const int m = e / KPS, cell = e - m * KPS;
+        const int r = cell / ROW, cc = cell - r * ROW;
+        const int gx = (x0 - 1 + cc + P.Nx) % P.Nx, gy = (y0 - 1 + r + P.Ny) % P.Ny;
+        goff[t] = (long long)min(m, 4) * P.sc + (long long)gy * P.sy + gx;
+    }
+    auto zw = [&](int z) { return z < 0 ? z + P.Nz : (z >= P.Nz ? z - P.Nz : z); };
+    auto issue = [&](int p) {
+        float* dst = ring + ((p + KRING) % KRING) * NE;
+        const float* src = q + (long long)zw(p) * P.sz;
+#pragma unroll
+        for (int t = 0; t < PER; ++t)
+            if (t < PER - 1 || tid + t * KPT < NE) cp_async4(dst + tid + t * KPT, src + goff[t]);
+    };
+    for (int p = z0 - 1; p <= z0 + 2; ++p) {
+        issue(p);
+        cp_async_commit();
+    }
+    const bool any_valid = valid[0] || valid[1];
+    for (int z = z0; z < z1; ++z) {
+        cp_async_wait<1>();  // planes z-1 .. z+1 are in
+        __syncthreads();     // every thread's copies visible; every thread done with plane z-2
+        if (z + 3 <= z1) issue(z + 3);
+        cp_async_commit();
+        if (any_valid) {
+            const float* pm = ring + ((z - 1 + KRING) % KRING) * NE + s_c;
+            const float* pc = ring + ((z + KRING) % KRING) * NE + s_c;
+            const float* pp = ring + ((z + 1) % KRING) * NE + s_c;
+            auto at = [](const float* b, int off) { return mk2(b[off], b[off + 4 * ROW]); };
+            F2 c[5], lap[5];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                const float* sc = pc + m * KPS;
+                c[m] = at(sc, 0);
+                lap[m] = vfma(P.ix2, at(sc, 1) + at(sc, -1),
+                              vfma(P.iy2, at(sc, ROW) + at(sc, -ROW),
+                                   vfma(P.iz2, at(pp + m * KPS, 0) + at(pm + m * KPS, 0), P.lap_c * c[m])));
+            }
+            F2 h[6];
+            bulk_field_pair(c, P.A, P.B, P.C, h);
+            h[0] = vfma(-P.kappa, lap[0], h[0]);
+            h[1] = vfma(-P.kappa, lap[3], h[1]);
+            h[2] = vfma(P.kappa, lap[0] + lap[3], h[2]);
+            h[3] = vfma(-P.kappa, lap[1], h[3]);
+            h[4] = vfma(-P.kappa, lap[2], h[4]);
+            h[5] = vfma(-P.kappa, lap[4], h[5]);
+            const F2 corr = (1.0f / 3.0f) * (h[0] + h[1] + h[2]);
+            const float nmd = -P.mob_dt;
+            F2 u[5] = {vfma(nmd, h[0] - corr, c[0]), vfma(nmd, h[3], c[1]), vfma(nmd, h[4], c[2]),
+                       vfma(nmd, h[1] - corr, c[3]), vfma(nmd, h[5], c[4])};
+            float v[2][5];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                v[0][m] = u[m].v.x;
+                v[1][m] = u[m].v.y;
+            }
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                if (!valid[r]) continue;
+                if (kNoise) {
+                    float g[5];
+                    normals5(cell_base[r] + (uint32_t)P.Nx * (uint32_t)P.Ny * (uint32_t)z, 0u, P.step, P.key0,
+                             P.key1, g);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) v[r][m] = fmaf(P.sigma, g[m], v[r][m]);
+                }
+                if (P.qcap > 0.0f) {
+                    const float zz = -v[r][0] - v[r][3];
+                    const float tr = v[r][0] * v[r][0] + v[r][3] * v[r][3] + zz * zz +
+                                     2.0f * (v[r][1] * v[r][1] + v[r][2] * v[r][2] + v[r][4] * v[r][4]);
+                    const float qn_ = sqrtf(fmaxf(tr, 0.0f));
+                    if (qn_ > P.qcap && qn_ > 0.0f) {
+                        const float sc = P.qcap / qn_;
+#pragma unroll
+                        for (int m = 0; m < 5; ++m) v[r][m] *= sc;
+                    }
+                }
+                float* o = out + (long long)z * P.sz + g_c[r];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) o[m * P.sc] = v[r][m];
+            }
+        }
+    }
+    cp_async_wait<0>();  // no copy into this CTA's shared memory outlives it
+}
+
 __global__ void k_kzm_from_aos(const double* __restrict__ aos, float* __restrict__ a, KzmConst P) {
     const long long n = (long long)P.Nx * P.Ny * P.Nz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -710,10 +830,15 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
     P.sigma = (float)a->noise_sigma;
     P.key0 = (uint32_t)a->seed;
     P.key1 = (uint32_t)(a->seed >> 32);
-    // Asynchronous-copy tiled kernel by default; LDG_KZM_KERNEL=direct selects the one-thread-per-
-    // site kernel, LDG_KZM_KERNEL=regs the register-queue tiled kernel.
+    // Two-site asynchronous-copy kernel by default; LDG_KZM_KERNEL=async selects the one-site
+    // asynchronous-copy kernel, =regs the register-queue tiled kernel, =direct the one-thread-per-
+    // site kernel.
     const char* ksel = getenv("LDG_KZM_KERNEL");
-    const int kind = (ksel && std::strcmp(ksel, "direct") == 0) ? 0 : ((ksel && std::strcmp(ksel, "regs") == 0) ? 1 : 2);
+    const int kind = !ksel                           ? 3
+                     : std::strcmp(ksel, "direct") == 0 ? 0
+                     : std::strcmp(ksel, "regs") == 0   ? 1
+                     : std::strcmp(ksel, "async") == 0  ? 2
+                                                        : 3;
     dim3 blk(32, 8, 1), grd((P.Nx + 31) / 32, (P.Ny + 7) / 8, P.Nz);
     dim3 tgrd((P.Nx + KTX - 1) / KTX, (P.Ny + KTY - 1) / KTY, (P.Nz + KZC - 1) / KZC);
     const size_t ring_bytes = (size_t)KRING * 5 * KPS * sizeof(float);
@@ -722,7 +847,10 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
         const bool noise = a->noise_sigma > 0.0;
         const float* in = h->q[h->cur];
         float* outb = h->q[1 - h->cur];
-        if (kind == 2) {
+        if (kind == 3) {
+            if (noise) k_kzm_step_pair<true><<<tgrd, KPT, ring_bytes, h->stream>>>(in, outb, P);
+            else k_kzm_step_pair<false><<<tgrd, KPT, ring_bytes, h->stream>>>(in, outb, P);
+        } else if (kind == 2) {
             if (noise) k_kzm_step_async<true><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
             else k_kzm_step_async<false><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
         } else if (kind == 1) {

@@ -69,9 +69,13 @@ def test_periodic_noise_statistics(oracle):
     assert np.array_equal(s.download() / sigma, z)
 
 
-@pytest.mark.parametrize("shape", [(64, 40, 70), (33, 17, 9), (2, 3, 4), (32, 8, 32)])
-def test_tiled_periodic_kernel_matches_direct(oracle, shape, monkeypatch):
-    # the z-marching tiled kernel (default) and the one-thread-per-site kernel agree, with noise
+@pytest.mark.parametrize("kernel", ["default", "async"])
+@pytest.mark.parametrize("shape", [(64, 40, 70), (33, 17, 9), (2, 3, 4), (32, 8, 32), (40, 13, 5)])
+def test_tiled_periodic_kernel_matches_direct(oracle, shape, kernel, monkeypatch):
+    # the z-marching tiled kernels (two sites per thread by default, one site per thread with
+    # LDG_KZM_KERNEL=async) and the one-thread-per-site kernel agree, with noise
+    if kernel != "default":
+        monkeypatch.setenv("LDG_KZM_KERNEL", kernel)
     A, B, C = bulk_ABC(0.044e6, 1.413e6, 1.153e6, 300.0, 307.0)
     bp, s = _pair(*shape, dy=1.1e-8)
     q0 = fp32(oracle.bulk_init(bp, 5, 0.05))
