@@ -575,8 +575,9 @@ def main():
         # strongly anchored cells) and reads the RHS of the moving cells
         alg_bytes += imex["jacobi"] * (40 * written + 20 * geo["evolving_cells"])
     achieved = alg_bytes / t_step / 1e9
-    # the committed DRAM traffic was captured with plain FP32 storage
-    traffic = None if (args.compensated or args.grid) else load_traffic(args.workload, alg_bytes)
+    # the committed DRAM traffic of each storage mode was captured at the workload's own size
+    traffic = None if args.grid else load_traffic(args.workload + ("+compensated" if args.compensated else ""),
+                                                  alg_bytes)
 
     e2e = None
     if not args.no_e2e:

@@ -307,17 +307,29 @@ __global__ void __launch_bounds__(KTX* KTY) k_kzm_step_async(const float* __rest
     cp_async_wait<0>();  // no copy into this CTA's shared memory outlives it
 }
 
-// Two sites per thread: the same tile, ring, copies and plane loop as k_kzm_step_async with
-// 128 threads, thread (tx, ty) updating rows ty and ty + 4 of the (32 x 8) tile. The Laplacian,
-// bulk field and update of both sites run as one packed FP32 instruction stream (FFMA2 / FADD2 /
-// FMUL2: per site the same fused operations as the one-site kernel); the noise draw, the cap and
-// the stores stay per site.
+// Two sites per thread: 128 threads over the same (32 x 8) tile and plane loop as
+// k_kzm_step_async, thread (tx, ty) updating rows ty and ty + 4. For Nx a multiple of 4 (so every
+// row pitch, plane pitch and component pitch is too) each ring row holds the 40 columns
+// x0 - 4 .. x0 + 35 and is fetched as ten 16-byte copies whose sources are 16-byte aligned and
+// either wholly inside the box or wholly wrapped (x0 is a multiple of 32): 500 copies per plane
+// instead of 1700 four-byte ones. The Laplacian, bulk field and update of both sites run as one
+// packed FP32 instruction stream (FFMA2 / FADD2 / FMUL2: per site the same fused operations as
+// the one-site kernel); the noise draw, the cap and the stores stay per site.
 constexpr int KPT = KTX * KTY / 2;
+constexpr int KROW2 = KTX + 8;               // ring row of the two-site kernel: x0 - 4 .. x0 + 35
+constexpr int KPS2 = (KTY + 2) * KROW2;      // floats per component plane
+constexpr size_t kRingBytes2 = (size_t)KRING * 5 * KPS2 * sizeof(float);
+__device__ __forceinline__ void cp_async16(float* sdst, const float* gsrc) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
 template <bool kNoise>
 __global__ void __launch_bounds__(KPT) k_kzm_step_pair(const float* __restrict__ q, float* __restrict__ out,
                                                        KzmConst P) {
-    extern __shared__ __align__(16) float ring[];  // [KRING][5][KTY+2][KTX+2]
-    constexpr int ROW = KTX + 2;
+    extern __shared__ __align__(16) float ring[];  // [KRING][5][KTY+2][KROW2]
+    constexpr int ROW = KROW2;
+    constexpr int KPS = KPS2;
     const int tid = threadIdx.x;
     const int tx = tid & 31, ty = tid >> 5;
     const int x0 = blockIdx.x * KTX, y0 = blockIdx.y * KTY, z0 = blockIdx.z * KZC;
@@ -335,17 +347,18 @@ __global__ void __launch_bounds__(KPT) k_kzm_step_pair(const float* __restrict__
         g_c[r] = (long long)y * P.sy + x;
         cell_base[r] = (uint32_t)(x + P.Nx * y);
     }
-    const int s_c = (ty + 1) * ROW + tx + 1;  // row ty; row ty + 4 is 4 * ROW further
-    constexpr int NE = 5 * KPS;
-    constexpr int PER = (NE + KPT - 1) / KPT;
+    const int s_c = (ty + 1) * ROW + tx + 4;  // row ty; row ty + 4 is 4 * ROW further
+    constexpr int NE = 5 * KPS;               // floats per ring plane
+    constexpr int NCH = NE / 4;               // 16-byte chunks per ring plane
+    constexpr int PER = (NCH + KPT - 1) / KPT;
     long long goff[PER];
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
-        const int e = tid + t * KPT;
-        const int m = e / KPS, cell = e - m * KPS;
-        const int r = cell / ROW, cc = cell - r * ROW;
-        const int gx = (x0 - 1 + cc + P.Nx) % P.Nx, gy = (y0 - 1 + r + P.Ny) % P.Ny;
-        goff[t] = (long long)min(m, 4) * P.sc + (long long)gy * P.sy + gx;
+        const int e = min(tid + t * KPT, NCH - 1);
+        const int m = e / (KPS / 4), rem = e - m * (KPS / 4);
+        const int r = rem / (ROW / 4), c4 = rem - r * (ROW / 4);
+        const int gx = (x0 - 4 + 4 * c4 + P.Nx) % P.Nx, gy = (y0 - 1 + r + P.Ny) % P.Ny;
+        goff[t] = (long long)m * P.sc + (long long)gy * P.sy + gx;
     }
     auto zw = [&](int z) { return z < 0 ? z + P.Nz : (z >= P.Nz ? z - P.Nz : z); };
     auto issue = [&](int p) {
@@ -353,7 +366,7 @@ __global__ void __launch_bounds__(KPT) k_kzm_step_pair(const float* __restrict__
         const float* src = q + (long long)zw(p) * P.sz;
 #pragma unroll
         for (int t = 0; t < PER; ++t)
-            if (t < PER - 1 || tid + t * KPT < NE) cp_async4(dst + tid + t * KPT, src + goff[t]);
+            if (t < PER - 1 || tid + t * KPT < NCH) cp_async16(dst + 4 * (tid + t * KPT), src + goff[t]);
     };
     for (int p = z0 - 1; p <= z0 + 2; ++p) {
         issue(p);
@@ -839,6 +852,8 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
                      : std::strcmp(ksel, "regs") == 0   ? 1
                      : std::strcmp(ksel, "async") == 0  ? 2
                                                         : 3;
+    // the two-site kernel's 16-byte copies need every pitch a multiple of 4 floats
+    const int kind_run = (kind == 3 && P.Nx % 4 != 0) ? 2 : kind;
     dim3 blk(32, 8, 1), grd((P.Nx + 31) / 32, (P.Ny + 7) / 8, P.Nz);
     dim3 tgrd((P.Nx + KTX - 1) / KTX, (P.Ny + KTY - 1) / KTY, (P.Nz + KZC - 1) / KZC);
     const size_t ring_bytes = (size_t)KRING * 5 * KPS * sizeof(float);
@@ -847,10 +862,10 @@ int kzm_step(kzm_handle* h, int n_steps, const kzm_step_args* a) {
         const bool noise = a->noise_sigma > 0.0;
         const float* in = h->q[h->cur];
         float* outb = h->q[1 - h->cur];
-        if (kind == 3) {
-            if (noise) k_kzm_step_pair<true><<<tgrd, KPT, ring_bytes, h->stream>>>(in, outb, P);
-            else k_kzm_step_pair<false><<<tgrd, KPT, ring_bytes, h->stream>>>(in, outb, P);
-        } else if (kind == 2) {
+        if (kind_run == 3) {
+            if (noise) k_kzm_step_pair<true><<<tgrd, KPT, kRingBytes2, h->stream>>>(in, outb, P);
+            else k_kzm_step_pair<false><<<tgrd, KPT, kRingBytes2, h->stream>>>(in, outb, P);
+        } else if (kind_run == 2) {
             if (noise) k_kzm_step_async<true><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
             else k_kzm_step_async<false><<<tgrd, blk, ring_bytes, h->stream>>>(in, outb, P);
         } else if (kind == 1) {
