@@ -77,8 +77,11 @@ __device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t 
     }
 }
 
-// Uniform in (0, 1] from a 21-bit integer.
-__device__ __forceinline__ float u21(uint32_t x) { return ((float)x + 1.0f) * (1.0f / 2097152.0f); }
+// Uniform in (0, 1] from a 21-bit integer: (x + 1) 2^-21, formed as one fused multiply-add
+// (exact: x is exact in FP32 and the result has at most 22 significant bits).
+__device__ __forceinline__ float u21(uint32_t x) {
+    return fmaf((float)x, 1.0f / 2097152.0f, 1.0f / 2097152.0f);
+}
 
 // Five standard normals for (cell, instance, step) from one Philox4x32-7 block: the four
 // 32-bit words give six disjoint 21-bit fields (the low 21 bits of each word, and the high
