@@ -717,8 +717,9 @@ struct TiledPlan {
 // the first changing cell (rounded down to the 4-float TMA alignment) instead of at multiples of
 // TK, and each tile's plane range is cut to the planes whose changing cells reach it: every
 // changing cell lies in exactly one item, and fewer idle lanes are visited than with a fixed tile
-// grid. Items are ordered with the plane chunk slowest (CTAs resident together share halo planes
-// in L2). *active: the cells of the grid inside the items' tiles (read once per step).
+// grid. Items are ordered longest first, and among items of one length with the plane chunk
+// slowest (CTAs resident together share halo planes in L2). *active: the cells of the grid inside
+// the items' tiles (read once per step).
 inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long* active) {
     using namespace tiled;
     std::vector<int4> items;
@@ -753,6 +754,10 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
         if (a.x != b.x) return a.x < b.x;
         return a.y < b.y;
     });
+    // Longest items first (ties keep the order above): CTAs are dispatched in item order, so
+    // the short items of the droplet's poles fill the last wave instead of trailing it.
+    std::stable_sort(items.begin(), items.end(),
+                     [](const int4& a, const int4& b) { return (a.w - a.z) > (b.w - b.z); });
     if (active) *active = act;
     return items;
 }
