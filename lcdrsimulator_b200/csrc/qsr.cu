@@ -204,6 +204,69 @@ __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ 
     for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
 }
 
+// The same sweep with two neighbouring cells per thread (k and k + 1, k even): the centre, i +- 1
+// and j +- 1 operands and the right-hand side of both cells are 8-byte loads, the k-neighbours
+// two 4-byte loads; 128 threads (16 pairs x 8 rows) per tile plane. Each cell's arithmetic is the
+// one-cell kernel's, operand for operand.
+template <bool kLast>
+__global__ void __launch_bounds__(128) k_jacobi_tiled2(const float* __restrict__ rhs, const float* __restrict__ qo,
+                                                       float* __restrict__ qn, const uint8_t* __restrict__ flags,
+                                                       const int4* __restrict__ items, QsrConst P) {
+    const int4 item = items[blockIdx.x];
+    const int i = item.z;
+    const int k = item.y + 2 * (int)(threadIdx.x & 15);  // even (tiles start at k0 = 2 mod 4)
+    const int j = item.x + (int)(threadIdx.x >> 4);
+    if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // the first tile of a row may start at k = -2
+    const long long id = (long long)i * P.si + (long long)j * P.sj + k;
+    const bool has1 = k + 1 < P.Nz;
+    const unsigned f2 = *reinterpret_cast<const unsigned short*>(flags + id);  // both cells' classes
+    const uint8_t f[2] = {(uint8_t)(f2 & 0xffu), has1 ? (uint8_t)(f2 >> 8) : (uint8_t)0};
+    bool wr[2], st[2];
+    const bool ij_face = (j == 0 || j == P.Ny - 1 || i == 0 || i == P.Nx - 1);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        wr[r] = (f[r] & (kMove | kFixed)) != 0;
+        const bool k_face = (k + r == 0) || (k + r == P.Nz - 1);
+        st[r] = wr[r] && !(kLast && (f[r] & kFixed)) && (f[r] & kMove) && !ij_face && !k_face;
+    }
+    if (!wr[0] && !wr[1]) return;
+    float o[2][5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const float* b = qo + m * P.sc + id;
+        const float2 c = *reinterpret_cast<const float2*>(b);
+        o[0][m] = c.x;
+        o[1][m] = c.y;
+        if (st[0] || st[1]) {  // i and j are interior here (ij_face is false)
+            const float2 xp = __ldg(reinterpret_cast<const float2*>(b + P.si));
+            const float2 xm = __ldg(reinterpret_cast<const float2*>(b - P.si));
+            const float2 yp = __ldg(reinterpret_cast<const float2*>(b + P.sj));
+            const float2 ym = __ldg(reinterpret_cast<const float2*>(b - P.sj));
+            const float km1 = k >= 1 ? __ldg(b - 1) : 0.0f;
+            const float kp2 = k + 2 < P.Nz ? __ldg(b + 2) : 0.0f;
+            const float2 rh = __ldg(reinterpret_cast<const float2*>(rhs + m * P.sc + id));
+            const float s0 = P.ix2 * (xp.x + xm.x) + P.iy2 * (yp.x + ym.x) + P.iz2 * (c.y + km1);
+            const float s1 = P.ix2 * (xp.y + xm.y) + P.iy2 * (yp.y + ym.y) + P.iz2 * (kp2 + c.x);
+            if (st[0]) o[0][m] = (rh.x + P.alpha * s0) * P.jdenom_inv;
+            if (st[1]) o[1][m] = (rh.y + P.alpha * s1) * P.jdenom_inv;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+        if (kLast && wr[r] && (f[r] & kFixed)) surface_q0(P, i, j, k + r, o[r]);
+    if (wr[0] && wr[1]) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(qn + m * P.sc + id) = make_float2(o[0][m], o[1][m]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+            if (wr[r]) {
+#pragma unroll
+                for (int m = 0; m < 5; ++m) qn[m * P.sc + id + r] = o[r][m];
+            }
+    }
+}
+
 // Host AoS FP64 (reference cell order) <-> device FP32 SoA.
 __global__ void k_aos_to_soa(const double* __restrict__ aos, float* __restrict__ a, float* __restrict__ b,
                              int Nx, int Ny, int Nz, int sj, long long si, long long sc, float* __restrict__ la = nullptr,
@@ -1091,7 +1154,21 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             int c = h->cur;
             for (int it = 0; it < a->jacobi_iters; ++it) {
                 const bool last = (it == a->jacobi_iters - 1);
-                if (tiled) {
+                static const bool pair2 = [] {
+                    const char* e = getenv("LDG_JACOBI_PAIR");
+                    return !(e && e[0] == '0');
+                }();
+                if (tiled && pair2) {
+                    if (h->tiled.n_plane_items > 0) {
+                        const int nb = h->tiled.n_plane_items;
+                        if (last)
+                            k_jacobi_tiled2<true><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                                                                             h->tiled.plane_items, P);
+                        else
+                            k_jacobi_tiled2<false><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                                                                              h->tiled.plane_items, P);
+                    }
+                } else if (tiled) {
                     if (h->tiled.n_plane_items > 0) {
                         const int nb = h->tiled.n_plane_items;
                         if (last)
