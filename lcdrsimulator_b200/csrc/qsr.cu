@@ -209,9 +209,9 @@ __global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ 
 // two 4-byte loads; 128 threads (16 pairs x 8 rows) per tile plane. Each cell's arithmetic is the
 // one-cell kernel's, operand for operand.
 template <bool kLast>
-__global__ void __launch_bounds__(128) k_jacobi_tiled2(const float* __restrict__ rhs, const float* __restrict__ qo,
-                                                       float* __restrict__ qn, const uint8_t* __restrict__ flags,
-                                                       const int4* __restrict__ items, QsrConst P) {
+__global__ void __launch_bounds__(128, 8) k_jacobi_tiled2(const float* __restrict__ rhs, const float* __restrict__ qo,
+                                                          float* __restrict__ qn, const uint8_t* __restrict__ flags,
+                                                          const int4* __restrict__ items, QsrConst P) {
     const int4 item = items[blockIdx.x];
     const int i = item.z;
     const int k = item.y + 2 * (int)(threadIdx.x & 15);  // even (tiles start at k0 = 2 mod 4)
@@ -219,25 +219,17 @@ __global__ void __launch_bounds__(128) k_jacobi_tiled2(const float* __restrict__
     if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // the first tile of a row may start at k = -2
     const long long id = (long long)i * P.si + (long long)j * P.sj + k;
     const bool has1 = k + 1 < P.Nz;
-    const unsigned f2 = *reinterpret_cast<const unsigned short*>(flags + id);  // both cells' classes
-    const uint8_t f[2] = {(uint8_t)(f2 & 0xffu), has1 ? (uint8_t)(f2 >> 8) : (uint8_t)0};
-    bool wr[2], st[2];
     const bool ij_face = (j == 0 || j == P.Ny - 1 || i == 0 || i == P.Nx - 1);
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        wr[r] = (f[r] & (kMove | kFixed)) != 0;
-        const bool k_face = (k + r == 0) || (k + r == P.Nz - 1);
-        st[r] = wr[r] && !(kLast && (f[r] & kFixed)) && (f[r] & kMove) && !ij_face && !k_face;
-    }
-    if (!wr[0] && !wr[1]) return;
-    float o[2][5];
+    // Every operand the stencil may need is loaded before the cell classes are known, so the
+    // loads of a thread go out together (one memory latency instead of two).
+    const unsigned f2 = __ldg(reinterpret_cast<const unsigned short*>(flags + id));  // both cells' classes
+    float2 c[5], s[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
         const float* b = qo + m * P.sc + id;
-        const float2 c = *reinterpret_cast<const float2*>(b);
-        o[0][m] = c.x;
-        o[1][m] = c.y;
-        if (st[0] || st[1]) {  // i and j are interior here (ij_face is false)
+        c[m] = __ldg(reinterpret_cast<const float2*>(b));
+        s[m] = make_float2(0.0f, 0.0f);
+        if (!ij_face) {
             const float2 xp = __ldg(reinterpret_cast<const float2*>(b + P.si));
             const float2 xm = __ldg(reinterpret_cast<const float2*>(b - P.si));
             const float2 yp = __ldg(reinterpret_cast<const float2*>(b + P.sj));
@@ -245,15 +237,23 @@ __global__ void __launch_bounds__(128) k_jacobi_tiled2(const float* __restrict__
             const float km1 = k >= 1 ? __ldg(b - 1) : 0.0f;
             const float kp2 = k + 2 < P.Nz ? __ldg(b + 2) : 0.0f;
             const float2 rh = __ldg(reinterpret_cast<const float2*>(rhs + m * P.sc + id));
-            const float s0 = P.ix2 * (xp.x + xm.x) + P.iy2 * (yp.x + ym.x) + P.iz2 * (c.y + km1);
-            const float s1 = P.ix2 * (xp.y + xm.y) + P.iy2 * (yp.y + ym.y) + P.iz2 * (kp2 + c.x);
-            if (st[0]) o[0][m] = (rh.x + P.alpha * s0) * P.jdenom_inv;
-            if (st[1]) o[1][m] = (rh.y + P.alpha * s1) * P.jdenom_inv;
+            const float s0 = P.ix2 * (xp.x + xm.x) + P.iy2 * (yp.x + ym.x) + P.iz2 * (c[m].y + km1);
+            const float s1 = P.ix2 * (xp.y + xm.y) + P.iy2 * (yp.y + ym.y) + P.iz2 * (kp2 + c[m].x);
+            s[m] = make_float2((rh.x + P.alpha * s0) * P.jdenom_inv, (rh.y + P.alpha * s1) * P.jdenom_inv);
         }
     }
+    const uint8_t f[2] = {(uint8_t)(f2 & 0xffu), has1 ? (uint8_t)(f2 >> 8) : (uint8_t)0};
+    bool wr[2];
+    float o[2][5];
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
+    for (int r = 0; r < 2; ++r) {
+        wr[r] = (f[r] & (kMove | kFixed)) != 0;
+        const bool k_face = (k + r == 0) || (k + r == P.Nz - 1);
+        const bool st = !(kLast && (f[r] & kFixed)) && (f[r] & kMove) && !ij_face && !k_face;
+#pragma unroll
+        for (int m = 0; m < 5; ++m) o[r][m] = st ? (r ? s[m].y : s[m].x) : (r ? c[m].y : c[m].x);
         if (kLast && wr[r] && (f[r] & kFixed)) surface_q0(P, i, j, k + r, o[r]);
+    }
     if (wr[0] && wr[1]) {
 #pragma unroll
         for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(qn + m * P.sc + id) = make_float2(o[0][m], o[1][m]);
