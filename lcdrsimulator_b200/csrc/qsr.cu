@@ -169,49 +169,15 @@ __global__ void __launch_bounds__(256) k_jacobi(const float* __restrict__ rhs, c
 // The same sweep over the tiles of the explicit step's work list only (tiles holding moving or
 // strongly anchored cells, each over its plane range), writing only moving and strongly anchored
 // cells. Every other cell never changes: it holds the same value in both ping-pong buffers, so
-// the reference's copy of it (QSR.cu:803-810) is already done. Block (32, 8) = one tile row per
-// warp; one block per visited tile plane (the work list expanded to single planes), so every
-// cell is an independent thread as in the full-box sweep and no block idles.
-static_assert(tiled::TK == 32 && tiled::TJ == 8, "k_jacobi_tiled maps one (8 x 32) tile onto a 256-thread block");
+// the reference's copy of it (QSR.cu:803-810) is already done. One block of 128 threads per
+// visited tile plane (the work list expanded to single planes); each thread updates two
+// neighbouring cells (k and k + 1, k even): the centre, i +- 1 and j +- 1 operands and the
+// right-hand side of both cells are 8-byte loads, the k-neighbours two 4-byte loads. Each cell's
+// arithmetic is the full-box sweep's, operand for operand.
 template <bool kLast>
-__global__ void __launch_bounds__(256) k_jacobi_tiled(const float* __restrict__ rhs, const float* __restrict__ qo,
-                                                      float* __restrict__ qn, const uint8_t* __restrict__ flags,
-                                                      const int4* __restrict__ items, QsrConst P) {
-    const int4 item = items[blockIdx.x];
-    const int i = item.z;
-    const int k = item.y + (int)(threadIdx.x & 31);
-    const int j = item.x + (int)(threadIdx.x >> 5);
-    if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // the first tile of a row may start at k = -2
-    const long long id = (long long)i * P.si + (long long)j * P.sj + k;
-    const uint8_t f = __ldg(flags + id);
-    if (!(f & (kMove | kFixed))) return;
-    float o[5];
-    if (kLast && (f & kFixed)) {
-        surface_q0(P, i, j, k, o);
-    } else if (j == 0 || k == 0 || j == P.Ny - 1 || k == P.Nz - 1 || i == 0 || i == P.Nx - 1 || !(f & kMove)) {
-#pragma unroll
-        for (int m = 0; m < 5; ++m) o[m] = __ldg(qo + m * P.sc + id);
-    } else {
-#pragma unroll
-        for (int m = 0; m < 5; ++m) {
-            const float* b = qo + m * P.sc + id;
-            const float s = P.ix2 * (__ldg(b + P.si) + __ldg(b - P.si)) +
-                            P.iy2 * (__ldg(b + P.sj) + __ldg(b - P.sj)) + P.iz2 * (__ldg(b + 1) + __ldg(b - 1));
-            o[m] = (__ldg(rhs + m * P.sc + id) + P.alpha * s) * P.jdenom_inv;
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < 5; ++m) qn[m * P.sc + id] = o[m];
-}
-
-// The same sweep with two neighbouring cells per thread (k and k + 1, k even): the centre, i +- 1
-// and j +- 1 operands and the right-hand side of both cells are 8-byte loads, the k-neighbours
-// two 4-byte loads; 128 threads (16 pairs x 8 rows) per tile plane. Each cell's arithmetic is the
-// one-cell kernel's, operand for operand.
-template <bool kLast>
-__global__ void __launch_bounds__(128, 8) k_jacobi_tiled2(const float* __restrict__ rhs, const float* __restrict__ qo,
-                                                          float* __restrict__ qn, const uint8_t* __restrict__ flags,
-                                                          const int4* __restrict__ items, QsrConst P) {
+__global__ void __launch_bounds__(128) k_jacobi_tiled(const float* __restrict__ rhs, const float* __restrict__ qo,
+                                                       float* __restrict__ qn, const uint8_t* __restrict__ flags,
+                                                       const int4* __restrict__ items, QsrConst P) {
     const int4 item = items[blockIdx.x];
     const int i = item.z;
     const int k = item.y + 2 * (int)(threadIdx.x & 15);  // even (tiles start at k0 = 2 mod 4)
@@ -219,17 +185,25 @@ __global__ void __launch_bounds__(128, 8) k_jacobi_tiled2(const float* __restric
     if (k < 0 || k >= P.Nz || j >= P.Ny) return;  // the first tile of a row may start at k = -2
     const long long id = (long long)i * P.si + (long long)j * P.sj + k;
     const bool has1 = k + 1 < P.Nz;
+    const unsigned f2 = *reinterpret_cast<const unsigned short*>(flags + id);  // both cells' classes
+    const uint8_t f[2] = {(uint8_t)(f2 & 0xffu), has1 ? (uint8_t)(f2 >> 8) : (uint8_t)0};
+    bool wr[2], st[2];
     const bool ij_face = (j == 0 || j == P.Ny - 1 || i == 0 || i == P.Nx - 1);
-    // Every operand the stencil may need is loaded before the cell classes are known, so the
-    // loads of a thread go out together (one memory latency instead of two).
-    const unsigned f2 = __ldg(reinterpret_cast<const unsigned short*>(flags + id));  // both cells' classes
-    float2 c[5], s[5];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        wr[r] = (f[r] & (kMove | kFixed)) != 0;
+        const bool k_face = (k + r == 0) || (k + r == P.Nz - 1);
+        st[r] = wr[r] && !(kLast && (f[r] & kFixed)) && (f[r] & kMove) && !ij_face && !k_face;
+    }
+    if (!wr[0] && !wr[1]) return;
+    float o[2][5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
         const float* b = qo + m * P.sc + id;
-        c[m] = __ldg(reinterpret_cast<const float2*>(b));
-        s[m] = make_float2(0.0f, 0.0f);
-        if (!ij_face) {
+        const float2 c = *reinterpret_cast<const float2*>(b);
+        o[0][m] = c.x;
+        o[1][m] = c.y;
+        if (st[0] || st[1]) {  // i and j are interior here (ij_face is false)
             const float2 xp = __ldg(reinterpret_cast<const float2*>(b + P.si));
             const float2 xm = __ldg(reinterpret_cast<const float2*>(b - P.si));
             const float2 yp = __ldg(reinterpret_cast<const float2*>(b + P.sj));
@@ -237,23 +211,15 @@ __global__ void __launch_bounds__(128, 8) k_jacobi_tiled2(const float* __restric
             const float km1 = k >= 1 ? __ldg(b - 1) : 0.0f;
             const float kp2 = k + 2 < P.Nz ? __ldg(b + 2) : 0.0f;
             const float2 rh = __ldg(reinterpret_cast<const float2*>(rhs + m * P.sc + id));
-            const float s0 = P.ix2 * (xp.x + xm.x) + P.iy2 * (yp.x + ym.x) + P.iz2 * (c[m].y + km1);
-            const float s1 = P.ix2 * (xp.y + xm.y) + P.iy2 * (yp.y + ym.y) + P.iz2 * (kp2 + c[m].x);
-            s[m] = make_float2((rh.x + P.alpha * s0) * P.jdenom_inv, (rh.y + P.alpha * s1) * P.jdenom_inv);
+            const float s0 = P.ix2 * (xp.x + xm.x) + P.iy2 * (yp.x + ym.x) + P.iz2 * (c.y + km1);
+            const float s1 = P.ix2 * (xp.y + xm.y) + P.iy2 * (yp.y + ym.y) + P.iz2 * (kp2 + c.x);
+            if (st[0]) o[0][m] = (rh.x + P.alpha * s0) * P.jdenom_inv;
+            if (st[1]) o[1][m] = (rh.y + P.alpha * s1) * P.jdenom_inv;
         }
     }
-    const uint8_t f[2] = {(uint8_t)(f2 & 0xffu), has1 ? (uint8_t)(f2 >> 8) : (uint8_t)0};
-    bool wr[2];
-    float o[2][5];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-        wr[r] = (f[r] & (kMove | kFixed)) != 0;
-        const bool k_face = (k + r == 0) || (k + r == P.Nz - 1);
-        const bool st = !(kLast && (f[r] & kFixed)) && (f[r] & kMove) && !ij_face && !k_face;
-#pragma unroll
-        for (int m = 0; m < 5; ++m) o[r][m] = st ? (r ? s[m].y : s[m].x) : (r ? c[m].y : c[m].x);
+    for (int r = 0; r < 2; ++r)
         if (kLast && wr[r] && (f[r] & kFixed)) surface_q0(P, i, j, k + r, o[r]);
-    }
     if (wr[0] && wr[1]) {
 #pragma unroll
         for (int m = 0; m < 5; ++m) *reinterpret_cast<float2*>(qn + m * P.sc + id) = make_float2(o[0][m], o[1][m]);
@@ -1154,29 +1120,15 @@ int qsr_step(qsr_handle* h, int n_steps, const qsr_step_args* a) {
             int c = h->cur;
             for (int it = 0; it < a->jacobi_iters; ++it) {
                 const bool last = (it == a->jacobi_iters - 1);
-                static const bool pair2 = [] {
-                    const char* e = getenv("LDG_JACOBI_PAIR");
-                    return !(e && e[0] == '0');
-                }();
-                if (tiled && pair2) {
+                if (tiled) {
                     if (h->tiled.n_plane_items > 0) {
                         const int nb = h->tiled.n_plane_items;
                         if (last)
-                            k_jacobi_tiled2<true><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                            k_jacobi_tiled<true><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
                                                                              h->tiled.plane_items, P);
                         else
-                            k_jacobi_tiled2<false><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
+                            k_jacobi_tiled<false><<<nb, 128, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
                                                                               h->tiled.plane_items, P);
-                    }
-                } else if (tiled) {
-                    if (h->tiled.n_plane_items > 0) {
-                        const int nb = h->tiled.n_plane_items;
-                        if (last)
-                            k_jacobi_tiled<true><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                            h->tiled.plane_items, P);
-                        else
-                            k_jacobi_tiled<false><<<nb, 256, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags,
-                                                                             h->tiled.plane_items, P);
                     }
                 } else if (last) {
                     k_jacobi<true><<<grd, blk, 0, h->stream>>>(h->rhs, h->q[c], h->q[1 - c], h->flags, P);
