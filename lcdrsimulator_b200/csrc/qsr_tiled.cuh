@@ -327,17 +327,21 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
     return ok;
 }
 
-// Shared-memory accessor of two cells of one plane: local (jl, kl) and (jl + 4, kl).
+// Rows of the two cells of a thread in the two-cell kernels: warp w updates tile rows
+// PAIR_R0 * w and PAIR_R0 * w + PAIR_DR.
+constexpr int PAIR_R0 = 1, PAIR_DR = 4;
+
+// Shared-memory accessor of two cells of one plane: local (jl, kl) and (jl + PAIR_DR, kl).
 struct SmemQ2 {
     const float* pl[5];
     int off;
     __device__ __forceinline__ F2 operator()(int c, int di, int dj, int dk) const {
         const float* s = pl[di + 2] + off + dj * RW + dk;
-        if (c < 5) return mk2(s[c * CSTR], s[c * CSTR + 4 * RW]);
-        return mk2(-(s[0] + s[3 * CSTR]), -(s[4 * RW] + s[3 * CSTR + 4 * RW]));
+        if (c < 5) return mk2(s[c * CSTR], s[c * CSTR + PAIR_DR * RW]);
+        return mk2(-(s[0] + s[3 * CSTR]), -(s[PAIR_DR * RW] + s[3 * CSTR + PAIR_DR * RW]));
     }
 };
-constexpr int PAIR_THREADS = TK * TJ / 2;  // 128: each thread updates rows jl and jl + 4 of the tile
+constexpr int PAIR_THREADS = TK * TJ / 2;  // 128: each thread updates two rows of the tile
 constexpr int PAIR_NWARP = PAIR_THREADS / 32;
 
 // process_tile for 128 threads, two cells per thread (rows w and w + 4 of warp w): the interior
@@ -392,7 +396,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
     uint8_t f_next[2];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-        jr[r] = j0 + w + 4 * r;
+        jr[r] = j0 + PAIR_R0 * w + PAIR_DR * r;
         in_grid[r] = (jr[r] < P.Ny) && (k >= 0) && (k < P.Nz);
         jk_int[r] = jr[r] >= kLo && jr[r] <= P.Ny - 1 - kLo && k >= kLo && k <= P.Nz - 1 - kLo;
         cell0[r] = (long long)jr[r] * P.sj + k;
@@ -433,7 +437,7 @@ __device__ __forceinline__ bool process_tile_pair(const CUtensorMap* tm, float* 
             for (int r = 0; r < 2; ++r) {
 #pragma unroll
                 for (int d = 0; d < 5; ++d) A[r].pl[d] = qpl[d];
-                A[r].off = (w + 4 * r + HJ) * RW + (kl + HK);
+                A[r].off = (PAIR_R0 * w + PAIR_DR * r + HJ) * RW + (kl + HK);
 #pragma unroll
                 for (int m = 0; m < 5; ++m) c[r][m] = A[r](m, 0, 0, 0);
             }
