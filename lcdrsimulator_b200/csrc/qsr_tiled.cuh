@@ -328,8 +328,10 @@ __device__ __forceinline__ bool process_tile(const CUtensorMap* tm, float* __res
 }
 
 // Rows of the two cells of a thread in the two-cell kernels: warp w updates tile rows
-// PAIR_R0 * w and PAIR_R0 * w + PAIR_DR.
-constexpr int PAIR_R0 = 1, PAIR_DR = 4;
+// PAIR_R0 * w and PAIR_R0 * w + PAIR_DR. Adjacent rows share operands: the centre of one cell
+// is a j-neighbour of the other, and their j +- 1 and j +- 2 rows overlap, so the compiler loads
+// those shared values once.
+constexpr int PAIR_R0 = 2, PAIR_DR = 1;
 
 // Shared-memory accessor of two cells of one plane: local (jl, kl) and (jl + PAIR_DR, kl).
 struct SmemQ2 {
@@ -344,7 +346,7 @@ struct SmemQ2 {
 constexpr int PAIR_THREADS = TK * TJ / 2;  // 128: each thread updates two rows of the tile
 constexpr int PAIR_NWARP = PAIR_THREADS / 32;
 
-// process_tile for 128 threads, two cells per thread (rows w and w + 4 of warp w): the interior
+// process_tile for 128 threads, two cells per thread (rows 2w and 2w + 1 of warp w): the interior
 // chemical potential of both cells runs as one packed (FFMA2 / FADD2 / FMUL2) instruction stream;
 // face cells, the strong-anchoring rewrite and the update run per cell.
 template <bool kL2, bool kL3, bool kNoise, bool kRHS, bool kComp = false>
