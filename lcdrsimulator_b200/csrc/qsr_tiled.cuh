@@ -79,14 +79,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
 }
-// One bounded try: the thread may sleep in the barrier until the phase completes or the hint
-// (1 ms) runs out, so a waiting warp takes no issue slots from the warps that still compute.
+// One bounded try: the thread may wait in the barrier for a system-dependent time before the
+// try returns false. (A suspend-time hint of 1 ms made the two-cell steps 1-2 % slower.)
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(su32(b)), "r"(parity), "r"(1000000u)
+        : "r"(su32(b)), "r"(parity)
         : "memory");
     return ok != 0;
 }
@@ -768,7 +768,8 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
     return items;
 }
 
-// Two cells per thread for the L2/L3 steps (LDG_QSR_PAIR=0 selects one cell per thread).
+// Two cells per thread for every explicit step and IMEX right-hand side (LDG_QSR_PAIR=0 selects
+// one cell per thread).
 inline bool tiled_pair_enabled() {
     static const bool on = [] {
         const char* e = getenv("LDG_QSR_PAIR");
@@ -896,7 +897,7 @@ inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const ui
         configured = true;
     }
     if (plan.n_items == 0) return LDG_OK;
-    if ((L2 || L3) && tiled_pair_enabled()) {
+    if (tiled_pair_enabled()) {
         const size_t smem2 = plan.smem_bytes[2];
         static bool configured_pair = false;
         if (!configured_pair) {
