@@ -768,14 +768,31 @@ inline std::vector<int4> tiled_items(const TiledPlan& plan, int chunk, long long
     return items;
 }
 
-// Two cells per thread for every explicit step and IMEX right-hand side (LDG_QSR_PAIR=0 selects
-// one cell per thread).
-inline bool tiled_pair_enabled() {
-    static const bool on = [] {
+// Kernel choice: LDG_QSR_PAIR=0 always takes one cell per thread, LDG_QSR_PAIR=1 always two;
+// otherwise (the default) the ensemble takes two and a single grid chooses by its work list.
+inline int tiled_pair_mode() {
+    static const int mode = [] {
         const char* e = getenv("LDG_QSR_PAIR");
-        return !(e && e[0] == '0');
+        return (e && e[0] == '0') ? 0 : ((e && e[0] == '1') ? 1 : 2);
     }();
-    return on;
+    return mode;
+}
+inline bool tiled_pair_enabled() { return tiled_pair_mode() != 0; }
+
+// A single grid takes the two-cell kernel when its work list fills the GPU at least twice over
+// (two waves of four 128-thread CTAs per SM); a smaller list finishes sooner with one cell per
+// thread, whose 256-thread CTAs bring twice the warps to each item (64^3, R = 28: 0.0102 against
+// 0.0123 ms per step).
+inline bool tiled_use_pair(const TiledPlan& plan) {
+    if (tiled_pair_mode() != 2) return tiled_pair_mode() == 1;
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess)
+            return 148;
+        return n;
+    }();
+    return plan.n_items >= 2 * 4 * sms;
 }
 
 inline int tiled_default_chunk() {
@@ -897,7 +914,7 @@ inline int tiled_launch_t(const TiledPlan& plan, int which, float* out, const ui
         configured = true;
     }
     if (plan.n_items == 0) return LDG_OK;
-    if (tiled_pair_enabled()) {
+    if (tiled_use_pair(plan)) {
         const size_t smem2 = plan.smem_bytes[2];
         static bool configured_pair = false;
         if (!configured_pair) {
