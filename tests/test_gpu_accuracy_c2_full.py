@@ -11,7 +11,7 @@ RMS |Q|, free energy relative to |F|.
 
 This relaxation from random directors passes through defect annihilations, where the dynamics
 amplifies any rounding-level difference: even compensated storage, 2e-8 from FP64 after 1k
-steps, is up to 7e-3 off at single cells at 25k steps (RMS 6e-6) and back to 1e-4 at 50k.
+steps, is up to 1e-3 off at single cells at 25k steps (RMS 7e-7) and back to 4e-5 at 50k.
 What holds at every check, and is asserted: compensated free energy <= 1e-8 and field RMS
 <= 1e-5, plain FP32 free energy <= 2e-7; compensated field max <= 1e-5 holds through 10k steps.
 
