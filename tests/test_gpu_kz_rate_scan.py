@@ -8,7 +8,7 @@ the reference tree, so this scan uses the periodic-quench physics of the benchma
 6e-12 N, gamma = 0.1, linear ramp 315 K -> 295 K over tau_Q steps, Langevin noise of strength
 kT/dx^3 at 300 K, initial |Q| ~ 1e-3) on a 64^3 box at the reference's explicit-limit dt, with
 five ramps tau_Q = 500 .. 8000 steps, each followed by a 2000-step hold at 295 K, and eight
-seeds per rate.
+seeds per rate (LDG_KZ_SCAN_N=128 runs it on a 128^3 box).
 
 Both sides start from the reference's own initial field (mt19937_64 Gaussian, seed per run) and
 follow the reference's temperature schedule; the noise streams differ (Philox4x32-7 here,
@@ -37,7 +37,8 @@ from lcdrsimulator_b200.physics import bulk_ABC, S_eq
 
 pytestmark = pytest.mark.gpu
 
-N, D, KAPPA, GAMMA = 64, 1e-8, 6e-12, 0.1
+# box edge: 64 in the default suite; LDG_KZ_SCAN_N=128 runs the same scan on a 128^3 box
+N, D, KAPPA, GAMMA = int(os.environ.get("LDG_KZ_SCAN_N", "64")), 1e-8, 6e-12, 0.1
 LDG = dict(a=0.044e6, b=1.413e6, c=1.153e6, T_star=307.0)
 T_HIGH, T_LOW, HOLD = 315.0, 295.0, 2000
 TAUS = [500, 1000, 2000, 4000, 8000]
@@ -113,7 +114,7 @@ def test_kz_rate_scan_slope_matches_reference_kernel(oracle):
                slope_reference_sd=sd_r, corr_reference=corr_r, published_slope=-0.515)
     out = os.environ.get("LDG_ACCURACY_OUT")
     if out:
-        with open(f"{out}.kz_rate_scan", "w") as f:
+        with open(f"{out}.kz_rate_scan" + ("" if N == 64 else f"_{N}"), "w") as f:
             json.dump(rec, f)
     n = len(SEEDS)
     for t, a, b in zip(TAUS, rows_o, rows_r):
